@@ -1,0 +1,328 @@
+"""Benchmark: single-position GPU perft throughput (leaf nodes/s) on B200.
+
+Workload: the position reached from the initial array by 4 uniformly random
+legal plies (splitmix64 seed 1, moves sorted by UCI text), perft depth 7
+without transposition tables.  One step = one whole perft(7) of that
+position on the GPU: host-driven BFS levels (make+count, decoupled look-back
+scan, shared-memory-staged generation) and the fused two-ply leaf kernel.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Printed JSON line (rank 0):
+  value    leaf nodes/s over all ranks, device time from CUDA events on the
+           engine stream (first kernel to last kernel of each step)
+  e2e      the same metric through the public C ABI call (pb_perft_position)
+           with the root in host memory: host->device copy of the root and
+           its moves and device->host read of the count inside the timed
+           region (host wall clock around the synchronous call)
+  roofline the leaf kernel against the integer-issue roofline
+  cpu_baseline  the reference's own -cpu path (oracle/_ref) on this host's
+           cores, one process per core over a sample of depth-2 subtrees
+With --gpus N > 1 (torchrun, one process per GPU) the depth-2 subtrees of the
+root are split over the ranks (strong scaling: total work fixed); the only
+exchange is one all-reduce of the per-rank counts.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {"workload": "single-position perft", "position": "4 random plies from the initial array, splitmix64 seed 1",
+            "depth": 7, "tt": False}
+METRIC = "leaf nodes/s"
+PROFILE_INST_PER_POSITION = None  # filled from profiles/ once ncu has measured it
+
+
+def _load_profile_constants():
+    path = os.path.join(ROOT, "profiles", "leaf_kernel_constants.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        med = statistics.median(sm) if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def flush_l2(torch, dev):
+    buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    buf.fill_(1)
+    del buf
+
+
+def depth2_subtrees(pg, root):
+    """The root's grandchildren (positions two plies down) in generation order."""
+    out = []
+    for m in pg.generate_moves(root):
+        c = pg.make_move(root, m)
+        for m2 in pg.generate_moves(c):
+            out.append(pg.make_move(c, m2))
+    return out
+
+
+def cpu_reference_sample(pg, root, depth, max_seconds=20.0, cores=None):
+    """The reference's -cpu path on this host: one process per core, each on a
+    depth-2 subtree (perft depth-2 of a grandchild), until the sample budget."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "perft_gpu_ref")
+    kind = "reference"
+    if not os.path.exists(ref):
+        return None
+    cores = cores or len(os.sched_getaffinity(0))
+    subs = depth2_subtrees(pg, root)
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    sub_depth = depth - 2
+    nodes, done = 0, 0
+    t0 = time.perf_counter()
+    i = 0
+    # waves of `cores` processes until the budget is spent
+    while i < len(subs) and time.perf_counter() - t0 < max_seconds:
+        wave = subs[i:i + cores]
+        procs = [subprocess.Popen([ref, pg.to_fen(s), str(sub_depth), "-cpu", "-nott"], stdout=subprocess.PIPE,
+                                  stderr=subprocess.DEVNULL, text=True, env=env) for s in wave]
+        for pr in procs:
+            out, _ = pr.communicate()
+            last = [l for l in out.splitlines() if l.startswith(f"Perft({sub_depth:02d})")]
+            if last:
+                nodes += int(last[0].split(":")[1].split(",")[0])
+                done += 1
+        i += cores
+    wall = time.perf_counter() - t0
+    return {"value": nodes / wall if wall > 0 else 0.0, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"{done} of {len(subs)} depth-2 subtrees of the bench position at perft {sub_depth} "
+                      f"(reference -cpu -nott, {cores} processes in parallel, {wall:.1f} s wall)",
+            "nodes": nodes, "seconds": wall}
+
+
+def run_reference_arm(args):
+    import perft_gpu_2026_b200 as pg
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    root = pg.config_position(4, 1)
+    vals = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_sample(pg, root, WORKLOAD["depth"], max_seconds=8.0)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/perft_gpu_ref not built"}))
+            return 0
+        if i >= args.warmup:
+            vals.append(r["value"])
+            last = r
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": last["seconds"] * 1e3,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": WORKLOAD,
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": last["cores"], "kind": "reference",
+                             "sample": last["sample"]},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--depth", type=int, default=WORKLOAD["depth"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import perft_gpu_2026_b200 as pg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    root = pg.config_position(4, 1)
+    depth = args.depth
+    eng = pg.Engine(device=local, use_tt=False)
+    eng.set_timing(True)
+
+    # shard: depth-2 subtrees round-robin over ranks (one rank: the whole root)
+    if world > 1:
+        subs = depth2_subtrees(pg, root)
+        mine = subs[rank::world]
+        sub_depth = depth - 2
+    else:
+        mine = [root]
+        sub_depth = depth
+
+    def step():
+        total, dev_ms, leaf_ms, leaf_pos, kernels, h2d, d2h = 0, 0.0, 0.0, 0, 0, 0, 0
+        for p in mine:
+            total += eng.perft_position(p, sub_depth)
+            st = eng.last_stats()
+            dev_ms += st.device_ms
+            leaf_ms += st.leaf_ms
+            leaf_pos += st.leaf_positions
+            kernels += st.kernels
+            h2d += st.h2d_bytes
+            d2h += st.d2h_bytes
+        return total, dev_ms, leaf_ms, leaf_pos, kernels, h2d, d2h
+
+    for _ in range(args.warmup):
+        step()
+    # timed region: device time from the engine's CUDA events per step
+    results = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush_l2(torch, dev)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            results.append(step())
+            torch.cuda.synchronize()
+    clocks = clk.summary()
+    nodes = results[0][0]
+    assert all(r[0] == nodes for r in results), "perft result changed between steps"
+    dev_ms = [r[1] for r in results]
+    leaf_ms = [r[2] for r in results]
+    my_ms = sum(dev_ms) / len(dev_ms)
+    my_leaf_ms = sum(leaf_ms) / len(leaf_ms)
+
+    # e2e: the public C-ABI call with the root in host memory, wall clock
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush_l2(torch, dev)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for p in mine:
+            eng.perft_position(p, sub_depth)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    my_e2e = statistics.median(e2e_ms)
+
+    if dist:
+        t = torch.tensor([my_ms, my_e2e, my_leaf_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        my_ms, my_e2e, my_leaf_ms = t.tolist()
+        c = torch.tensor([nodes], dtype=torch.int64, device=dev)
+        dist.all_reduce(c)
+        nodes = int(c.item())
+    if rank == 0:
+        peaks, peak_kind = _peaks()
+        consts = _load_profile_constants()
+        leaf_pos = results[0][3]
+        kernels = results[0][4]
+        sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+        issue_peak = 148 * 4 * sm_mhz * 1e6 / 1e9  # G warp-instructions / s
+        inst_per_pos = consts.get("warp_inst_per_position")
+        roofline = {"bound": "int_issue", "unit": "Gwarp-inst/s", "peak": issue_peak,
+                    "peak_source": f"148 SMs x 4 issue/clk x sm_max_mhz ({peak_kind})",
+                    "kernel": "k_leaf2", "leaf_ms": my_leaf_ms, "positions_per_launch": leaf_pos,
+                    "positions_per_s": leaf_pos / (my_leaf_ms / 1e3) if my_leaf_ms > 0 else None,
+                    "achieved": None, "frac": None, "traffic": consts.get("dram_bytes_per_launch")}
+        if inst_per_pos:
+            ach = inst_per_pos * leaf_pos / (my_leaf_ms / 1e3) / 1e9
+            roofline["achieved"] = ach
+            roofline["frac"] = ach / issue_peak
+            roofline["inst_per_position"] = inst_per_pos
+        line = {"metric": METRIC, "value": nodes / (my_ms / 1e3), "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": my_ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": dict(WORKLOAD, depth=depth, nodes=nodes, l2="flushed (256 MB write) before each step",
+                               parallelism=f"depth-2 subtrees over {world} rank(s)"),
+                "e2e": {"value": nodes / (my_e2e / 1e3), "unit": METRIC, "ms_per_step": my_e2e,
+                        "h2d_bytes_per_step": int(results[0][5]), "d2h_bytes_per_step": int(results[0][6]),
+                        "timing": "host wall clock around pb_perft_position"},
+                "gpu_launches": int(kernels), "clocks": clocks, "roofline": roofline}
+        if world == 1 and not args.no_cpu_baseline:
+            cb = cpu_reference_sample(pg, root, depth, max_seconds=15.0)
+            if cb:
+                line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line))
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,157 @@
+/*
+ * perft_b200.h - C ABI of the B200 perft engine (libperftb200.so).
+ *
+ * The reference (perft_gpu) has no library API: its boundary is the
+ * perft_gpu command line (perft.cu:13-186) over an internal C++ function set
+ * (launcher.h:13-35).  Each entry point below names the reference function it
+ * stands in for.  All calls are synchronous, return a PB_* status code and
+ * never exit the process; a context owns its device memory and stream and is
+ * used from one host thread at a time.  Counts are bit-exact with the
+ * reference's `-cpu` path (launcher.cu:762-816) on the same FEN and depth.
+ */
+#ifndef PERFT_B200_H
+#define PERFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PB_OK = 0,
+    PB_ERR_ARG = -1,        /* bad argument (null pointer, depth out of range) */
+    PB_ERR_FEN = -2,        /* FEN rejected (see pb_parse_fen) */
+    PB_ERR_CUDA = -3,       /* a CUDA call failed; pb_last_error has the text */
+    PB_ERR_NOMEM = -4,      /* device or host allocation failed */
+    PB_ERR_DEVICE = -5,     /* a kernel reported an error word (timeout, capacity) */
+    PB_ERR_NODEVICE = -6    /* no CUDA device (GPU entry points only) */
+};
+
+/* Position: quad bitboard (chess.h:66-76) + packed state byte (castle bits
+ * [3:0] = white K,Q black K,Q; en-passant file+1 in [7:4], chess.h:78-92) +
+ * side to move (0 white, 1 black). 40 bytes. */
+typedef struct {
+    uint64_t bb[4];
+    uint8_t state;
+    uint8_t color;
+    uint8_t pad[6];
+} pb_pos;
+
+typedef struct {
+    uint64_t lo, hi;
+} pb_u128;
+
+typedef struct {
+    size_t arena_bytes;   /* BFS arena; 0 = auto (launcher.cu:59-88 sizes it from VRAM) */
+    int use_tt;           /* transposition tables on (-nott clears it, perft.cu:26-29) */
+    int device_tt_mb;     /* -dtt: device TT budget in MB, 0 = auto */
+    int host_tt_mb;       /* -htt: host TT budget in MB, 0 = auto */
+    int launch_depth;     /* -ld: GPU/CPU split depth, 0 = auto (launcher.cu:533-562) */
+    int strict;           /* 1 = exact counts where the reference's counting merges moves */
+    int verbose;          /* print allocation lines like the reference's preamble */
+} pb_opts;
+
+typedef struct pb_ctx pb_ctx;
+
+/* Library version string. */
+const char *pb_version(void);
+
+/* Fills opts with defaults (TT on, auto budgets, auto launch depth). */
+void pb_default_opts(pb_opts *opts);
+
+/* Replaces initGPU + initMoveGen + initTT (launcher.cu:59-88, :128-351;
+ * perft_kernels.cu:995-1134). device < 0 creates a host-only context (the
+ * -cpu mode, perft.cu:100-116). */
+int pb_create(int device, const pb_opts *opts, pb_ctx **out);
+
+/* Replaces freeTT + cudaFree of the arena (launcher.cu:509-531, perft.cu:180-181). */
+void pb_destroy(pb_ctx *ctx);
+
+/* Text of the last error on this context (never NULL). */
+const char *pb_last_error(const pb_ctx *ctx);
+
+/* Replaces readFENString (util.cpp:7-95).  The halfmove/fullmove fields are
+ * ignored like the reference.  Unlike the reference, positions a legal game
+ * cannot reach are rejected (missing or extra king, adjacent kings, side not
+ * to move in check, pawns on the first/last rank), castle rights without the
+ * king and rook on their home squares are dropped, and an en-passant square
+ * without a pawn that just double-pushed is dropped. */
+int pb_parse_fen(const char *fen, pb_pos *out);
+
+/* Writes the FEN of pos into buf (at least 96 bytes). */
+int pb_to_fen(const pb_pos *pos, char *buf, size_t len);
+
+/* Number of CUDA devices (cudaGetDeviceCount, perft.cu:62-69); 0 if none. */
+int pb_device_count(void);
+
+/* Fixes the launch depth used by pb_perft_launch for this context and
+ * returns it: opts.launch_depth when set, else estimated from the branching
+ * factor of pos and the arena size (estimateLaunchDepth, launcher.cu:533-562). */
+int pb_choose_launch_depth(pb_ctx *ctx, const pb_pos *pos);
+
+/* Replaces perft_gpu_host_bfs (perft_kernels.cu:620-990): perft(depth) of one
+ * position, the whole subtree on the GPU (the host only splits the root when
+ * a level would not fit the arena). */
+int pb_perft_position(pb_ctx *ctx, const pb_pos *pos, int depth, uint64_t *count);
+
+/* Replaces perftLauncher (launcher.cu:718-737): perft(depth) with the tree
+ * above the launch depth walked on the host (with the host TT when enabled)
+ * and GPU calls below it.  128-bit result. */
+int pb_perft_launch(pb_ctx *ctx, const pb_pos *pos, int depth, pb_u128 *count, double *seconds);
+
+/* The CLI loop (perft.cu:156-177): perft for depths 1..max_depth of a FEN,
+ * cumulative per-depth results and wall times. */
+int pb_perft(pb_ctx *ctx, const char *fen, int max_depth, pb_u128 *per_depth, double *per_depth_secs);
+
+/* Replaces perft_cpu_dispatch (launcher.cu:807-816): host-only perft. */
+int pb_perft_cpu(pb_ctx *ctx, const pb_pos *pos, int depth, uint64_t *count);
+
+/* No reference counterpart: perft of n independent roots in one batched GPU
+ * pass; counts[i] = perft(depths[i]) of roots[i]. */
+int pb_perft_batch(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uint64_t *counts);
+
+/* Host chess core (MoveGeneratorBitboard.h:1700-2067): legal-move count with
+ * the reference's counting conventions (strict = 0) or exact (strict = 1),
+ * move generation (returns the number of moves written, buffer >= 256) and
+ * make-move. */
+int pb_count_moves(const pb_pos *pos, int strict);
+int pb_generate_moves(const pb_pos *pos, uint16_t *moves);
+int pb_make_move(pb_pos *pos, uint16_t move);
+
+/* Workload generator (no reference counterpart): a playout of `plies`
+ * uniformly random legal moves from the standard initial array; each move is
+ * drawn with splitmix64 (state advanced in place) among the legal moves sorted
+ * by UCI text.  Returns the number of plies played (fewer at mate/stalemate). */
+int pb_random_playout(uint64_t *rng_state, int plies, pb_pos *out);
+
+/* Statistics of the last GPU perft call on a context.  The device times are
+ * CUDA events on the context's stream; no reference counterpart (the
+ * reference keeps host-timer histograms behind VERBOSE_LOGGING,
+ * launcher.cu:35-57). */
+typedef struct {
+    double device_ms;          /* first kernel to last kernel, engine stream */
+    double leaf_ms;            /* the fused two-ply leaf kernel alone */
+    uint64_t leaf_edges;       /* edges the leaf kernel took (one perft(2) each) */
+    uint64_t leaf_positions;   /* positions the leaf kernel counted (move-count calls) */
+    uint64_t nodes;            /* the perft result of the call */
+    uint32_t kernels;          /* kernel launches of the call */
+    uint32_t levels;           /* BFS expand levels */
+    uint64_t level_sizes[16];  /* edges per level, level 0 = root moves */
+    uint64_t h2d_bytes;        /* host-to-device bytes copied */
+    uint64_t d2h_bytes;        /* device-to-host bytes copied */
+} pb_stats;
+
+/* Turns per-call event timing on or off (off by default). */
+int pb_set_timing(pb_ctx *ctx, int enable);
+int pb_last_stats(const pb_ctx *ctx, pb_stats *out);
+
+/* Device kernels on caller-owned device buffers, for tests: exclusive scan of
+ * n u32 counts into n u64 offsets and a device u64 total. */
+int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

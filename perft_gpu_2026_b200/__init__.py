@@ -1,0 +1,328 @@
+"""perft_gpu_2026_b200 - Python binding of the B200 perft engine.
+
+The engine is the native library ``libperftb200.so`` (CUDA kernels for sm_100a
+plus a C++ host driver) behind the C ABI declared in ``include/perft_b200.h``.
+This module loads it with ctypes and mirrors the reference's operator set:
+
+    perft_gpu <fen> <depth> [-nott] [-dtt MB] [-htt MB] [-ld N] [-cpu]   (perft.cu:13-186)
+
+``Engine.perft`` is the per-depth loop, ``Engine.perft_position`` the single
+GPU breadth-first call (perft_gpu_host_bfs, perft_kernels.cu:620-990) and
+``Engine.perft_cpu`` the host path (perft_cpu_dispatch, launcher.cu:807-816).
+There is no Python fallback: if the library is missing the import fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import List, Optional, Sequence, Tuple
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libperftb200.so")
+
+START_FEN = "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1"
+
+PB_OK = 0
+PB_ERR_ARG = -1
+PB_ERR_FEN = -2
+PB_ERR_CUDA = -3
+PB_ERR_NOMEM = -4
+PB_ERR_DEVICE = -5
+PB_ERR_NODEVICE = -6
+
+
+class Pos(ctypes.Structure):
+    """pb_pos: quad bitboard + state byte + side to move (40 bytes)."""
+
+    _fields_ = [
+        ("bb", ctypes.c_uint64 * 4),
+        ("state", ctypes.c_uint8),
+        ("color", ctypes.c_uint8),
+        ("pad", ctypes.c_uint8 * 6),
+    ]
+
+    def key(self) -> Tuple[int, int, int, int, int, int]:
+        return (self.bb[0], self.bb[1], self.bb[2], self.bb[3], self.state, self.color)
+
+
+class U128(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_uint64), ("hi", ctypes.c_uint64)]
+
+    def value(self) -> int:
+        return (self.hi << 64) | self.lo
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [
+        ("arena_bytes", ctypes.c_size_t),
+        ("use_tt", ctypes.c_int),
+        ("device_tt_mb", ctypes.c_int),
+        ("host_tt_mb", ctypes.c_int),
+        ("launch_depth", ctypes.c_int),
+        ("strict", ctypes.c_int),
+        ("verbose", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    """pb_stats: per-call statistics (CUDA-event device times, sizes, launches)."""
+
+    _fields_ = [
+        ("device_ms", ctypes.c_double),
+        ("leaf_ms", ctypes.c_double),
+        ("leaf_edges", ctypes.c_uint64),
+        ("leaf_positions", ctypes.c_uint64),
+        ("nodes", ctypes.c_uint64),
+        ("kernels", ctypes.c_uint32),
+        ("levels", ctypes.c_uint32),
+        ("level_sizes", ctypes.c_uint64 * 16),
+        ("h2d_bytes", ctypes.c_uint64),
+        ("d2h_bytes", ctypes.c_uint64),
+    ]
+
+
+class PerftError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"perft engine error {code}: {msg}")
+        self.code = code
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m perft_gpu_2026_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    sig = {
+        "pb_version": (ctypes.c_char_p, []),
+        "pb_default_opts": (None, [P(Opts)]),
+        "pb_create": (ctypes.c_int, [ctypes.c_int, P(Opts), P(ctypes.c_void_p)]),
+        "pb_destroy": (None, [ctypes.c_void_p]),
+        "pb_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+        "pb_parse_fen": (ctypes.c_int, [ctypes.c_char_p, P(Pos)]),
+        "pb_to_fen": (ctypes.c_int, [P(Pos), ctypes.c_char_p, ctypes.c_size_t]),
+        "pb_perft_position": (ctypes.c_int, [ctypes.c_void_p, P(Pos), ctypes.c_int, P(ctypes.c_uint64)]),
+        "pb_perft_launch": (ctypes.c_int, [ctypes.c_void_p, P(Pos), ctypes.c_int, P(U128), P(ctypes.c_double)]),
+        "pb_perft": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, P(U128), P(ctypes.c_double)]),
+        "pb_perft_cpu": (ctypes.c_int, [ctypes.c_void_p, P(Pos), ctypes.c_int, P(ctypes.c_uint64)]),
+        "pb_perft_batch": (ctypes.c_int, [ctypes.c_void_p, P(Pos), P(ctypes.c_int), ctypes.c_int, P(ctypes.c_uint64)]),
+        "pb_count_moves": (ctypes.c_int, [P(Pos), ctypes.c_int]),
+        "pb_generate_moves": (ctypes.c_int, [P(Pos), P(ctypes.c_uint16)]),
+        "pb_make_move": (ctypes.c_int, [P(Pos), ctypes.c_uint16]),
+        "pb_random_playout": (ctypes.c_int, [P(ctypes.c_uint64), ctypes.c_int, P(Pos)]),
+        "pb_device_count": (ctypes.c_int, []),
+        "pb_choose_launch_depth": (ctypes.c_int, [ctypes.c_void_p, P(Pos)]),
+        "pb_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+        "pb_last_stats": (ctypes.c_int, [ctypes.c_void_p, P(Stats)]),
+        "pb_dev_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_LIB = None
+
+
+class _LazyLib:
+    """Loads libperftb200.so on first use; raises ImportError if it is not built."""
+
+    def __getattr__(self, name):
+        global _LIB
+        if _LIB is None:
+            _LIB = _load()
+        return getattr(_LIB, name)
+
+
+lib = _LazyLib()
+
+
+def device_count() -> int:
+    return lib.pb_device_count()
+
+
+def version() -> str:
+    return lib.pb_version().decode()
+
+
+def parse_fen(fen: str) -> Pos:
+    p = Pos()
+    rc = lib.pb_parse_fen(fen.encode(), ctypes.byref(p))
+    if rc != PB_OK:
+        raise PerftError(rc, f"invalid FEN: {fen!r}")
+    return p
+
+
+def to_fen(p: Pos) -> str:
+    buf = ctypes.create_string_buffer(128)
+    lib.pb_to_fen(ctypes.byref(p), buf, 128)
+    return buf.value.decode()
+
+
+def count_moves(p: Pos, strict: bool = False) -> int:
+    return lib.pb_count_moves(ctypes.byref(p), int(strict))
+
+
+def generate_moves(p: Pos) -> List[int]:
+    buf = (ctypes.c_uint16 * 256)()
+    n = lib.pb_generate_moves(ctypes.byref(p), buf)
+    return list(buf[:n])
+
+
+def make_move(p: Pos, move: int) -> Pos:
+    q = Pos()
+    ctypes.memmove(ctypes.byref(q), ctypes.byref(p), ctypes.sizeof(Pos))
+    lib.pb_make_move(ctypes.byref(q), move)
+    return q
+
+
+def move_uci(m: int) -> str:
+    f, t, fl = m & 63, (m >> 6) & 63, m >> 12
+    s = "abcdefgh"[f & 7] + str(1 + (f >> 3)) + "abcdefgh"[t & 7] + str(1 + (t >> 3))
+    if fl & 8:
+        s += "nbrq"[fl & 3]
+    return s
+
+
+def random_playout(seed_state: int, plies: int) -> Tuple[Pos, int, int]:
+    """Returns (position, plies played, advanced generator state)."""
+    st = ctypes.c_uint64(seed_state)
+    p = Pos()
+    n = lib.pb_random_playout(ctypes.byref(st), plies, ctypes.byref(p))
+    return p, n, st.value
+
+
+def splitmix64(state: int) -> Tuple[int, int]:
+    """One splitmix64 step in Python: returns (value, new state)."""
+    m = (1 << 64) - 1
+    state = (state + 0x9E3779B97F4A7C15) & m
+    z = state
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    return z ^ (z >> 31), state
+
+
+@dataclass
+class Workload:
+    """A named set of root positions with their perft depths."""
+
+    name: str
+    roots: List[Pos]
+    depths: List[int]
+
+
+def config_position(plies: int, seed: int) -> Pos:
+    """A position reached by `plies` random legal moves from the initial array."""
+    p, _, _ = random_playout(seed, plies)
+    return p
+
+
+def uneven_roots(n: int, lo: int, hi: int, seed: int) -> List[Pos]:
+    """n roots from playouts of U[lo, hi] plies, drawn from one splitmix64
+    stream (length draw, then the moves), keeping roots with a legal move."""
+    out: List[Pos] = []
+    st = seed
+    span = hi - lo + 1
+    while len(out) < n:
+        r, st = splitmix64(st)
+        plies = lo + ((r * span) >> 64)
+        c = ctypes.c_uint64(st)
+        p = Pos()
+        lib.pb_random_playout(ctypes.byref(c), plies, ctypes.byref(p))
+        st = c.value
+        if lib.pb_count_moves(ctypes.byref(p), 1) > 0:
+            out.append(p)
+    return out
+
+
+class Engine:
+    """A perft context on one device (device < 0: host only, the -cpu mode)."""
+
+    def __init__(self, device: int = 0, use_tt: bool = False, arena_bytes: int = 0, strict: bool = False,
+                 launch_depth: int = 0, device_tt_mb: int = 0, host_tt_mb: int = 0, verbose: bool = False):
+        o = Opts()
+        lib.pb_default_opts(ctypes.byref(o))
+        o.use_tt = int(use_tt)
+        o.arena_bytes = arena_bytes
+        o.strict = int(strict)
+        o.launch_depth = launch_depth
+        o.device_tt_mb = device_tt_mb
+        o.host_tt_mb = host_tt_mb
+        o.verbose = int(verbose)
+        h = ctypes.c_void_p()
+        rc = lib.pb_create(device, ctypes.byref(o), ctypes.byref(h))
+        if rc != PB_OK:
+            raise PerftError(rc, "pb_create failed")
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self._h:
+            lib.pb_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        if rc != PB_OK:
+            raise PerftError(rc, lib.pb_last_error(self._h).decode())
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def perft_position(self, p: Pos, depth: int) -> int:
+        out = ctypes.c_uint64()
+        self._check(lib.pb_perft_position(self._h, ctypes.byref(p), depth, ctypes.byref(out)))
+        return out.value
+
+    def perft_launch(self, p: Pos, depth: int) -> Tuple[int, float]:
+        out = U128()
+        secs = ctypes.c_double()
+        self._check(lib.pb_perft_launch(self._h, ctypes.byref(p), depth, ctypes.byref(out), ctypes.byref(secs)))
+        return out.value(), secs.value
+
+    def perft(self, fen: str, max_depth: int) -> List[Tuple[int, float]]:
+        res = (U128 * max_depth)()
+        secs = (ctypes.c_double * max_depth)()
+        self._check(lib.pb_perft(self._h, fen.encode(), max_depth, res, secs))
+        return [(res[i].value(), secs[i]) for i in range(max_depth)]
+
+    def perft_cpu(self, p: Pos, depth: int) -> int:
+        out = ctypes.c_uint64()
+        self._check(lib.pb_perft_cpu(self._h, ctypes.byref(p), depth, ctypes.byref(out)))
+        return out.value
+
+    def perft_batch(self, roots: Sequence[Pos], depths: Sequence[int]) -> List[int]:
+        n = len(roots)
+        arr = (Pos * n)(*roots)
+        d = (ctypes.c_int * n)(*depths)
+        out = (ctypes.c_uint64 * n)()
+        self._check(lib.pb_perft_batch(self._h, arr, d, n, out))
+        return list(out)
+
+    def set_timing(self, enable: bool = True) -> None:
+        self._check(lib.pb_set_timing(self._h, int(enable)))
+
+    def last_stats(self) -> Stats:
+        st = Stats()
+        self._check(lib.pb_last_stats(self._h, ctypes.byref(st)))
+        return st
+
+    def choose_launch_depth(self, p: Pos) -> int:
+        return lib.pb_choose_launch_depth(self._h, ctypes.byref(p))
+
+    def dev_scan(self, d_in: int, n: int, d_out: int, d_total: int) -> None:
+        self._check(lib.pb_dev_scan(self._h, ctypes.c_void_p(d_in), n, ctypes.c_void_p(d_out), ctypes.c_void_p(d_total)))

@@ -1,0 +1,649 @@
+// pb_engine.cu - host driver and C ABI of the B200 perft engine.
+//
+// Single translation unit: the tables, the kernels and the host code are
+// compiled together so the __device__ tables have one definition.
+//
+// Call structure (reference equivalents in brackets):
+//   pb_create            device init, table upload, arena   [initGPU, initMoveGen]
+//   pb_perft             per-depth loop over pb_perft_launch [perft.cu main loop]
+//   pb_perft_launch      host recursion above the launch depth, host TT
+//                        [perftLauncher / perft_cpu_recurse]
+//   pb_perft_position    one GPU breadth-first perft          [perft_gpu_host_bfs]
+//   pb_perft_cpu         host-only perft                     [perft_cpu_dispatch]
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <string>
+#include <vector>
+
+#include "../../include/perft_b200.h"
+#include "pb_tables.cuh"
+#include "pb_util.cuh"
+#include "pb_kernels.cuh"
+#include "pb_tt.cuh"
+
+using namespace pb;
+
+#define PB_VERSION "perft-b200 0.1"
+
+struct pb_ctx {
+    int device = -1;
+    bool gpu = false;
+    pb_opts opts{};
+    cudaStream_t stream = nullptr;
+    char *arena = nullptr;
+    size_t arena_bytes = 0;
+    // small device scratch: counter, error word, scan ticket, level total
+    unsigned long long *d_counter = nullptr;
+    u32 *d_err = nullptr;
+    u32 *d_ticket = nullptr;
+    u64 *d_total = nullptr;
+    u64 *h_pinned = nullptr;  // pinned host words for readbacks
+    int launch_depth = 0;
+    bool timing = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // call start, leaf start, leaf end, call end
+    pb_stats stats{};
+    HostTT htt;
+    DeviceTT dtt;
+    std::string err;
+};
+
+namespace {
+
+int fail(pb_ctx *ctx, int code, const std::string &msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(pb_ctx *ctx, cudaError_t e, const char *what)
+{
+    return fail(ctx, PB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PB_CUDA(call)                                        \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+inline Board to_board(const pb_pos &p)
+{
+    Board b;
+    for (int i = 0; i < 4; i++) b.bb[i] = p.bb[i];
+    return b;
+}
+inline void to_pos(const Board &b, u32 st, int color, pb_pos &p)
+{
+    memset(&p, 0, sizeof(p));
+    for (int i = 0; i < 4; i++) p.bb[i] = b.bb[i];
+    p.state = (uint8_t)st;
+    p.color = (uint8_t)color;
+}
+
+// ---------------------------------------------------------------- host core wrappers
+u32 host_count(const Board &b, u32 st, int c, bool strict)
+{
+    if (c == WHITE) return strict ? count_moves<WHITE, true>(b, st) : count_moves<WHITE, false>(b, st);
+    return strict ? count_moves<BLACK, true>(b, st) : count_moves<BLACK, false>(b, st);
+}
+int host_gen(const Board &b, u32 st, int c, uint16_t *out)
+{
+    ArraySink s{out, 0};
+    if (c == WHITE)
+        gen_moves<WHITE>(b, st, s);
+    else
+        gen_moves<BLACK>(b, st, s);
+    return s.n;
+}
+void host_make(Board &b, u32 &st, int c, uint16_t m)
+{
+    if (c == WHITE)
+        make_move<WHITE>(b, st, m);
+    else
+        make_move<BLACK>(b, st, m);
+}
+
+u64 host_perft(const Board &b, u32 st, int c, int depth, bool strict)
+{
+    if (depth <= 0) return 1;
+    if (depth == 1) return host_count(b, st, c, strict);
+    uint16_t mv[MAX_MOVES];
+    int n = host_gen(b, st, c, mv);
+    u64 total = 0;
+    for (int i = 0; i < n; i++) {
+        Board cb = b;
+        u32 cs = st;
+        host_make(cb, cs, c, mv[i]);
+        total += host_perft(cb, cs, 1 - c, depth - 1, strict);
+    }
+    return total;
+}
+
+// ---------------------------------------------------------------- arena
+struct Arena {
+    char *base;
+    size_t cap, off = 0;
+    template <class T> T *take(u64 n)
+    {
+        size_t bytes = ((size_t)n * sizeof(T) + 255) & ~(size_t)255;
+        if (off + bytes > cap) return nullptr;
+        T *p = reinterpret_cast<T *>(base + off);
+        off += bytes;
+        return p;
+    }
+};
+
+inline unsigned grid_for(u64 n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+enum { BFS_OK = 0, BFS_TOO_BIG = 1 };
+
+// One GPU breadth-first perft; status BFS_TOO_BIG when a level would not fit.
+int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth, u64 *out, int *bfs_status)
+{
+    *bfs_status = BFS_OK;
+    const bool strict = ctx->opts.strict != 0;
+    if (depth <= 2) {
+        *out = host_perft(root, root_st, color, depth, strict);
+        return PB_OK;
+    }
+    uint16_t root_moves[MAX_MOVES];
+    int n0 = host_gen(root, root_st, color, root_moves);
+    if (n0 == 0) {
+        *out = 0;
+        return PB_OK;
+    }
+    cudaStream_t s = ctx->stream;
+    pb_stats &stats = ctx->stats;
+    Arena ar{ctx->arena, ctx->arena_bytes};
+    Board *pb_ = ar.take<Board>(1);
+    uint8_t *ps = ar.take<uint8_t>(1);
+    uint16_t *emv = ar.take<uint16_t>(n0);
+    u32 *epi = ar.take<u32>(n0);
+    if (!pb_ || !ps || !emv || !epi) {
+        *bfs_status = BFS_TOO_BIG;
+        return PB_OK;
+    }
+    uint8_t st8 = (uint8_t)root_st;
+    PB_CUDA(cudaMemcpyAsync(pb_, &root, sizeof(Board), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(ps, &st8, 1, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(emv, root_moves, sizeof(uint16_t) * n0, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemsetAsync(epi, 0, sizeof(u32) * n0, s));
+    PB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s));
+    stats.h2d_bytes += sizeof(Board) + 1 + sizeof(uint16_t) * n0;
+    if (stats.levels < 16) stats.level_sizes[stats.levels] = (u64)n0;
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[0], s));
+
+    Board *cur_b = pb_;
+    uint8_t *cur_s = ps;
+    u64 n = (u64)n0;
+    int c = color;
+    for (int rem = depth - 1; rem > 2; rem--) {
+        Board *cb = ar.take<Board>(n);
+        uint8_t *cs = ar.take<uint8_t>(n);
+        u32 *cnt = ar.take<u32>(n);
+        u64 *offs = ar.take<u64>(n);
+        u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+        u64 *status = ar.take<u64>(tiles);
+        if (!cb || !cs || !cnt || !offs || !status) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        if (c == WHITE)
+            k_expand_count<WHITE><<<grid_for(n, 256), 256, 0, s>>>(cur_b, cur_s, epi, emv, n, cb, cs, cnt);
+        else
+            k_expand_count<BLACK><<<grid_for(n, 256), 256, 0, s>>>(cur_b, cur_s, epi, emv, n, cb, cs, cnt);
+        PB_CUDA(cudaGetLastError());
+        PB_CUDA(cudaMemsetAsync(status, 0, sizeof(u64) * tiles, s));
+        PB_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s));
+        k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(cnt, n, offs, status, ctx->d_ticket, ctx->d_total, ctx->d_err);
+        PB_CUDA(cudaGetLastError());
+        PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_total, sizeof(u64), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 1, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+        stats.kernels += 2;
+        stats.d2h_bytes += 12;
+        if ((u32)ctx->h_pinned[1]) return fail(ctx, PB_ERR_DEVICE, "scan reported a device error");
+        u64 next = ctx->h_pinned[0];
+        stats.levels++;
+        if (stats.levels < 16) stats.level_sizes[stats.levels] = next;
+        if (next == 0) {
+            *out = 0;
+            return PB_OK;
+        }
+        if (next > 0xFFFFFFFFULL) {  // parent indices are u32
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        uint16_t *nmv = ar.take<uint16_t>(next);
+        u32 *npi = ar.take<u32>(next);
+        if (!nmv || !npi) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        if (c == WHITE)
+            k_generate<BLACK><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n, nmv, npi);
+        else
+            k_generate<WHITE><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n, nmv, npi);
+        PB_CUDA(cudaGetLastError());
+        stats.kernels += 1;
+        cur_b = cb;
+        cur_s = cs;
+        emv = nmv;
+        epi = npi;
+        n = next;
+        c = 1 - c;
+    }
+    PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(unsigned long long), s));
+    unsigned g = grid_for(n, 256);
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[1], s));
+    if (c == WHITE) {
+        if (strict)
+            k_leaf2<WHITE, true><<<g, 256, 0, s>>>(cur_b, cur_s, epi, emv, n, ctx->d_counter);
+        else
+            k_leaf2<WHITE, false><<<g, 256, 0, s>>>(cur_b, cur_s, epi, emv, n, ctx->d_counter);
+    } else {
+        if (strict)
+            k_leaf2<BLACK, true><<<g, 256, 0, s>>>(cur_b, cur_s, epi, emv, n, ctx->d_counter);
+        else
+            k_leaf2<BLACK, false><<<g, 256, 0, s>>>(cur_b, cur_s, epi, emv, n, ctx->d_counter);
+    }
+    PB_CUDA(cudaGetLastError());
+    if (ctx->timing) {
+        PB_CUDA(cudaEventRecord(ctx->ev[2], s));
+        PB_CUDA(cudaEventRecord(ctx->ev[3], s));
+    }
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_counter, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 2, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    if ((u32)ctx->h_pinned[2]) return fail(ctx, PB_ERR_DEVICE, "kernel reported a device error");
+    *out = ctx->h_pinned[0];
+    stats.kernels += 1;
+    stats.leaf_edges += n;
+    stats.leaf_positions += ctx->h_pinned[1];
+    stats.d2h_bytes += 20;
+    if (ctx->timing) {
+        float a = 0, b2 = 0;
+        PB_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[3]));
+        PB_CUDA(cudaEventElapsedTime(&b2, ctx->ev[1], ctx->ev[2]));
+        stats.device_ms += a;
+        stats.leaf_ms += b2;
+    }
+    return PB_OK;
+}
+
+// perft of one position on the GPU; a level too big for the arena splits the
+// root on the host and recurses (the reference's OOM path recomputes one
+// level down the same way, launcher.cu:600-610, but on the CPU).
+int gpu_perft(pb_ctx *ctx, const Board &b, u32 st, int c, int depth, u64 *out)
+{
+    int status = BFS_OK;
+    int rc = bfs_perft(ctx, b, st, c, depth, out, &status);
+    if (rc != PB_OK) return rc;
+    if (status == BFS_OK) return PB_OK;
+    if (depth <= 3) return fail(ctx, PB_ERR_NOMEM, "BFS arena too small for a depth-3 perft");
+    uint16_t mv[MAX_MOVES];
+    int n = host_gen(b, st, c, mv);
+    u64 total = 0;
+    for (int i = 0; i < n; i++) {
+        Board cb = b;
+        u32 cs = st;
+        host_make(cb, cs, c, mv[i]);
+        u64 sub = 0;
+        rc = gpu_perft(ctx, cb, cs, 1 - c, depth - 1, &sub);
+        if (rc != PB_OK) return rc;
+        total += sub;
+    }
+    *out = total;
+    return PB_OK;
+}
+
+// ---------------------------------------------------------------- 128-bit helpers
+inline void add128(pb_u128 &a, const pb_u128 &b)
+{
+    u64 old = a.lo;
+    a.lo += b.lo;
+    a.hi += b.hi + (a.lo < old ? 1 : 0);
+}
+
+// Host recursion above the launch depth (perft_cpu_recurse, launcher.cu:572-715).
+int launch_recurse(pb_ctx *ctx, const Board &b, u32 st, int c, int depth, const Hash128 &h, pb_u128 *out)
+{
+    const bool tt = ctx->opts.use_tt && ctx->htt.ready();
+    if (tt && depth >= 2) {
+        u64 hit;
+        if (ctx->htt.probe(depth, h, &hit)) {
+            out->lo = hit;
+            out->hi = 0;
+            return PB_OK;
+        }
+    }
+    pb_u128 total{0, 0};
+    if (depth <= ctx->launch_depth) {
+        u64 v = 0;
+        int rc = ctx->gpu ? gpu_perft(ctx, b, st, c, depth, &v) : PB_OK;
+        if (rc != PB_OK) return rc;
+        if (!ctx->gpu) v = host_perft(b, st, c, depth, ctx->opts.strict != 0);
+        total.lo = v;
+    } else {
+        uint16_t mv[MAX_MOVES];
+        int n = host_gen(b, st, c, mv);
+        for (int i = 0; i < n; i++) {
+            Board cb = b;
+            u32 cs = st;
+            host_make(cb, cs, c, mv[i]);
+            Hash128 ch = tt ? hash_move(h, b, st, cs, c, mv[i]) : Hash128{0, 0};
+            pb_u128 sub;
+            int rc = launch_recurse(ctx, cb, cs, 1 - c, depth - 1, ch, &sub);
+            if (rc != PB_OK) return rc;
+            add128(total, sub);
+        }
+    }
+    if (tt && depth >= 2 && total.hi == 0) ctx->htt.store(depth, h, total.lo);
+    *out = total;
+    return PB_OK;
+}
+
+// Launch depth: the deepest GPU call whose BFS levels fit half the arena,
+// from the root's branching factor (estimateLaunchDepth, launcher.cu:533-562).
+int estimate_launch_depth(pb_ctx *ctx, const Board &b, u32 st, int c)
+{
+    double p1 = (double)host_perft(b, st, c, 1, true);
+    double p2 = (double)host_perft(b, st, c, 2, true);
+    double p3 = (double)host_perft(b, st, c, 3, true);
+    if (p1 < 1 || p2 < 1 || p3 < 1) return 6;
+    double bf = 0.5 * (sqrt((p3 / p2) * (p2 / p1)) + 0.5 * ((p3 / p2) + (p2 / p1)));
+    bf = std::max(bf, 2.0);
+    // a GPU call of depth L materialises about bf^(L-2) edges of ~6 B and
+    // bf^(L-3) positions of ~45 B; allow a factor 4 for uneven subtrees
+    double budget = (double)ctx->arena_bytes / 4.0;
+    int ld = 3;
+    for (int L = 4; L <= 12; L++) {
+        double need = 6.0 * pow(bf, L - 2) + 45.0 * pow(bf, L - 3);
+        if (need > budget) break;
+        ld = L;
+    }
+    return std::max(ld, 4);
+}
+
+}  // namespace
+
+// ==================================================================== C ABI
+extern "C" {
+
+const char *pb_version(void) { return PB_VERSION; }
+
+void pb_default_opts(pb_opts *o)
+{
+    memset(o, 0, sizeof(*o));
+    o->use_tt = 1;
+}
+
+int pb_create(int device, const pb_opts *opts, pb_ctx **out)
+{
+    if (!out) return PB_ERR_ARG;
+    *out = nullptr;
+    if (!build_host_tables()) return PB_ERR_ARG;
+    pb_ctx *ctx = new pb_ctx();
+    if (opts)
+        ctx->opts = *opts;
+    else
+        pb_default_opts(&ctx->opts);
+    ctx->device = device;
+    if (device >= 0) {
+        int count = 0;
+        cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count == 0 || device >= count) {
+            delete ctx;
+            return PB_ERR_NODEVICE;
+        }
+        ctx->gpu = true;
+        int rc = PB_OK;
+        do {
+            if ((e = cudaSetDevice(device)) != cudaSuccess) { rc = cuda_fail(ctx, e, "cudaSetDevice"); break; }
+            if ((e = cudaMemcpyToSymbol(g_tab, &h_tab, sizeof(Tables))) != cudaSuccess) { rc = cuda_fail(ctx, e, "upload tables"); break; }
+            if ((e = cudaMemcpyToSymbol(g_attacks, h_attacks, sizeof(h_attacks))) != cudaSuccess) { rc = cuda_fail(ctx, e, "upload attacks"); break; }
+            if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = cuda_fail(ctx, e, "stream"); break; }
+            char *small = nullptr;
+            if ((e = cudaMalloc(&small, 256)) != cudaSuccess) { rc = cuda_fail(ctx, e, "scratch"); break; }
+            ctx->d_counter = reinterpret_cast<unsigned long long *>(small);  // two words
+            ctx->d_err = reinterpret_cast<u32 *>(small + 64);
+            ctx->d_ticket = reinterpret_cast<u32 *>(small + 128);
+            ctx->d_total = reinterpret_cast<u64 *>(small + 192);
+            if ((e = cudaMallocHost(&ctx->h_pinned, 64)) != cudaSuccess) { rc = cuda_fail(ctx, e, "pinned"); break; }
+            size_t freeb = 0, totalb = 0;
+            cudaMemGetInfo(&freeb, &totalb);
+            size_t want = ctx->opts.arena_bytes;
+            if (!want) {
+                // no TT: half of free memory up to 32 GiB; TT mode keeps room for the tables
+                size_t cap = ctx->opts.use_tt ? (16ULL << 30) : (32ULL << 30);
+                want = std::min(freeb / 2, cap);
+            }
+            if ((e = cudaMalloc(&ctx->arena, want)) != cudaSuccess) { rc = cuda_fail(ctx, e, "arena"); break; }
+            ctx->arena_bytes = want;
+            if (ctx->opts.use_tt) {
+                rc = ctx->dtt.init(ctx->opts.device_tt_mb, freeb > want ? freeb - want : 0, ctx->opts.verbose, &ctx->err);
+                if (rc != PB_OK) break;
+            }
+        } while (0);
+        if (rc != PB_OK) {
+            std::string msg = ctx->err;
+            pb_destroy(ctx);
+            return rc;
+        }
+        if (ctx->opts.verbose)
+            printf("Allocated BFS buffer: %llu MB\n", (unsigned long long)(ctx->arena_bytes >> 20));
+    }
+    *out = ctx;
+    return PB_OK;
+}
+
+void pb_destroy(pb_ctx *ctx)
+{
+    if (!ctx) return;
+    if (ctx->gpu) {
+        cudaSetDevice(ctx->device);
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        ctx->dtt.release();
+        for (int i = 0; i < 4; i++)
+            if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+        if (ctx->arena) cudaFree(ctx->arena);
+        if (ctx->d_counter) cudaFree(ctx->d_counter);
+        if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+}
+
+const char *pb_last_error(const pb_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int pb_parse_fen(const char *fen, pb_pos *out)
+{
+    if (!fen || !out) return PB_ERR_ARG;
+    build_host_tables();
+    return parse_fen(fen, out) ? PB_OK : PB_ERR_FEN;
+}
+
+int pb_to_fen(const pb_pos *pos, char *buf, size_t len)
+{
+    if (!pos || !buf || len < 96) return PB_ERR_ARG;
+    write_fen(*pos, buf);
+    return PB_OK;
+}
+
+int pb_count_moves(const pb_pos *pos, int strict)
+{
+    if (!pos) return PB_ERR_ARG;
+    build_host_tables();
+    return (int)host_count(to_board(*pos), pos->state, pos->color, strict != 0);
+}
+
+int pb_generate_moves(const pb_pos *pos, uint16_t *moves)
+{
+    if (!pos || !moves) return PB_ERR_ARG;
+    build_host_tables();
+    return host_gen(to_board(*pos), pos->state, pos->color, moves);
+}
+
+int pb_make_move(pb_pos *pos, uint16_t move)
+{
+    if (!pos) return PB_ERR_ARG;
+    Board b = to_board(*pos);
+    u32 st = pos->state;
+    host_make(b, st, pos->color, move);
+    to_pos(b, st, 1 - pos->color, *pos);
+    return PB_OK;
+}
+
+int pb_perft_cpu(pb_ctx *ctx, const pb_pos *pos, int depth, uint64_t *count)
+{
+    if (!pos || !count || depth < 0) return PB_ERR_ARG;
+    build_host_tables();
+    bool strict = ctx ? ctx->opts.strict != 0 : false;
+    *count = host_perft(to_board(*pos), pos->state, pos->color, depth, strict);
+    return PB_OK;
+}
+
+int pb_perft_position(pb_ctx *ctx, const pb_pos *pos, int depth, uint64_t *count)
+{
+    if (!ctx || !pos || !count || depth < 0 || depth > 20) return PB_ERR_ARG;
+    if (!ctx->gpu) return fail(ctx, PB_ERR_NODEVICE, "context has no GPU");
+    PB_CUDA(cudaSetDevice(ctx->device));
+    memset(&ctx->stats, 0, sizeof(ctx->stats));
+    int rc = gpu_perft(ctx, to_board(*pos), pos->state, pos->color, depth, reinterpret_cast<u64 *>(count));
+    ctx->stats.nodes = *count;
+    return rc;
+}
+
+int pb_set_timing(pb_ctx *ctx, int enable)
+{
+    if (!ctx || !ctx->gpu) return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    if (enable && !ctx->ev[0])
+        for (int i = 0; i < 4; i++) PB_CUDA(cudaEventCreate(&ctx->ev[i]));
+    ctx->timing = enable != 0;
+    return PB_OK;
+}
+
+int pb_last_stats(const pb_ctx *ctx, pb_stats *out)
+{
+    if (!ctx || !out) return PB_ERR_ARG;
+    *out = ctx->stats;
+    return PB_OK;
+}
+
+int pb_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+int pb_choose_launch_depth(pb_ctx *ctx, const pb_pos *pos)
+{
+    if (!ctx || !pos) return PB_ERR_ARG;
+    build_host_tables();
+    if (!ctx->launch_depth)
+        ctx->launch_depth = ctx->opts.launch_depth > 0
+                                ? ctx->opts.launch_depth
+                                : (ctx->gpu ? estimate_launch_depth(ctx, to_board(*pos), pos->state, pos->color) : 64);
+    return ctx->launch_depth;
+}
+
+int pb_perft_launch(pb_ctx *ctx, const pb_pos *pos, int depth, pb_u128 *count, double *seconds)
+{
+    if (!ctx || !pos || !count || depth < 0 || depth > 30) return PB_ERR_ARG;
+    if (ctx->gpu) PB_CUDA(cudaSetDevice(ctx->device));
+    Board b = to_board(*pos);
+    pb_choose_launch_depth(ctx, pos);
+    if (ctx->opts.use_tt && !ctx->htt.ready()) ctx->htt.init(ctx->opts.host_tt_mb, ctx->launch_depth, depth);
+    auto t0 = std::chrono::steady_clock::now();
+    pb_u128 r{0, 0};
+    int rc;
+    if (depth == 0) {
+        r.lo = 1;
+        rc = PB_OK;
+    } else {
+        Hash128 h = ctx->opts.use_tt ? hash_position(b, pos->state, pos->color) : Hash128{0, 0};
+        rc = launch_recurse(ctx, b, pos->state, pos->color, depth, h, &r);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    *count = r;
+    return rc;
+}
+
+int pb_perft(pb_ctx *ctx, const char *fen, int max_depth, pb_u128 *per_depth, double *per_depth_secs)
+{
+    if (!ctx || !fen || !per_depth || max_depth < 1 || max_depth > 30) return PB_ERR_ARG;
+    pb_pos pos;
+    if (!parse_fen(fen, &pos)) return fail(ctx, PB_ERR_FEN, "invalid FEN");
+    for (int d = 1; d <= max_depth; d++) {
+        double secs = 0;
+        int rc = pb_perft_launch(ctx, &pos, d, &per_depth[d - 1], &secs);
+        if (rc != PB_OK) return rc;
+        if (per_depth_secs) per_depth_secs[d - 1] = secs;
+    }
+    return PB_OK;
+}
+
+int pb_random_playout(uint64_t *rng_state, int plies, pb_pos *out)
+{
+    if (!rng_state || !out || plies < 0) return PB_ERR_ARG;
+    build_host_tables();
+    parse_fen("rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1", out);
+    int played = 0;
+    for (int i = 0; i < plies; i++) {
+        uint16_t mv[MAX_MOVES];
+        int n = pb_generate_moves(out, mv);
+        if (n <= 0) break;
+        std::vector<std::pair<std::string, uint16_t>> keyed;
+        keyed.reserve(n);
+        for (int k = 0; k < n; k++) keyed.emplace_back(move_uci(mv[k]), mv[k]);
+        std::sort(keyed.begin(), keyed.end());
+        u64 r = splitmix64(reinterpret_cast<u64 *>(rng_state));
+        u32 pick = (u32)(((unsigned __int128)r * (u32)n) >> 64);
+        pb_make_move(out, keyed[pick].second);
+        played++;
+    }
+    return played;
+}
+
+int pb_perft_batch(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uint64_t *counts)
+{
+    if (!ctx || !roots || !depths || !counts || n < 0) return PB_ERR_ARG;
+    if (!ctx->gpu) return fail(ctx, PB_ERR_NODEVICE, "context has no GPU");
+    PB_CUDA(cudaSetDevice(ctx->device));
+    for (int i = 0; i < n; i++) {
+        int rc = gpu_perft(ctx, to_board(roots[i]), roots[i].state, roots[i].color, depths[i], reinterpret_cast<u64 *>(&counts[i]));
+        if (rc != PB_OK) return rc;
+    }
+    return PB_OK;
+}
+
+int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total)
+{
+    if (!ctx || !ctx->gpu || !d_in || !d_out || !d_total) return PB_ERR_ARG;
+    if (n == 0) return PB_OK;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    Arena ar{ctx->arena, ctx->arena_bytes};
+    u64 *status = ar.take<u64>(tiles);
+    if (!status) return fail(ctx, PB_ERR_NOMEM, "arena too small for scan status");
+    PB_CUDA(cudaMemsetAsync(status, 0, sizeof(u64) * tiles, s));
+    PB_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s));
+    PB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s));
+    k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(d_in, n, reinterpret_cast<u64 *>(d_out), status, ctx->d_ticket, reinterpret_cast<u64 *>(d_total), ctx->d_err);
+    PB_CUDA(cudaGetLastError());
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 1, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    if ((u32)ctx->h_pinned[1]) return fail(ctx, PB_ERR_DEVICE, "scan reported a device error");
+    return PB_OK;
+}
+
+}  // extern "C"

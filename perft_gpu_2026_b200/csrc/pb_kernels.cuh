@@ -1,0 +1,285 @@
+// pb_kernels.cuh - sm_100a kernels of the breadth-first perft engine.
+//
+// A BFS level is a list of edges (parent index u32, move u16) over the
+// previous level's positions (Board 32 B + state 1 B, structure of arrays).
+// Per level the host launches
+//   k_expand_count  make each edge's move, store the child position and its
+//                   exact legal-move count
+//   k_scan_*        decoupled look-back exclusive scan of the counts (u64)
+//   k_generate      write every child's moves as the next level's edges,
+//                   staged through shared memory so global stores coalesce
+// and the last two plies run in k_leaf2 (fused: make, generate, then count
+// every grandchild).  These replace, in order, the reference's
+// makemove_and_count_moves_kernel (perft_kernels.cu:201-257), CUB
+// InclusiveSum (:786), merge_path_partitions + mp_interval_expand_kernel +
+// generate_moves_kernel (:77-173, :263-311) and fused_2level_leaf_kernel
+// (:405-480).  The interval expand (child slot -> parent index) is done
+// inside k_generate: each parent writes its own index next to each of its
+// moves in the shared-memory tile, so no separate search pass is needed.
+#pragma once
+#include "pb_core.cuh"
+
+namespace pb {
+
+// 256-bit position load/store (one ld/st.global.v4.u64 on sm_100).
+__device__ __forceinline__ Board load_board(const Board *p)
+{
+    Board b;
+    asm volatile("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(b.bb[0]), "=l"(b.bb[1]), "=l"(b.bb[2]), "=l"(b.bb[3])
+                 : "l"(p));
+    return b;
+}
+__device__ __forceinline__ void store_board(Board *p, const Board &b)
+{
+    asm volatile("st.global.v4.u64 [%0], {%1,%2,%3,%4};" ::"l"(p), "l"(b.bb[0]), "l"(b.bb[1]), "l"(b.bb[2]),
+                 "l"(b.bb[3])
+                 : "memory");
+}
+
+// Device-side error word: kernels OR a code in and return instead of trapping.
+enum : u32 {
+    DEVERR_SCAN_TIMEOUT = 1u,
+    DEVERR_CAPACITY = 2u,
+};
+
+// ---------------------------------------------------------------- expand/count
+// Child c of edge e: board/state written at index e, count[e] = exact number
+// of moves of the child (side to move 1-C).
+template <int C>
+__global__ void __launch_bounds__(256) k_expand_count(const Board *__restrict__ pboards,
+                                                      const uint8_t *__restrict__ pstates,
+                                                      const u32 *__restrict__ pidx,
+                                                      const uint16_t *__restrict__ moves, u64 n,
+                                                      Board *__restrict__ cboards, uint8_t *__restrict__ cstates,
+                                                      u32 *__restrict__ counts)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    u32 p = pidx[i];
+    Board b = load_board(pboards + p);
+    u32 st = pstates[p];
+    make_move<C>(b, st, moves[i]);
+    store_board(cboards + i, b);
+    cstates[i] = (uint8_t)st;
+    counts[i] = count_moves<1 - C, true>(b, st);
+}
+
+// ---------------------------------------------------------------- scan
+// Decoupled look-back exclusive scan of u32 counts into u64 offsets; the
+// grand total lands in *total.  Tile status words: [63:62] flag (1 = tile
+// aggregate, 2 = inclusive prefix), [61:0] value.  Tiles are taken in launch
+// order from an atomic ticket so every predecessor is already resident.
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr u64 ST_AGG = 1ULL << 62, ST_PREFIX = 2ULL << 62, ST_VALUE = (1ULL << 62) - 1;
+constexpr u32 SCAN_SPIN_LIMIT = 1u << 22;
+
+__device__ __forceinline__ void st_release(u64 *p, u64 v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ u64 ld_acquire(const u64 *p)
+{
+    u64 v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan(const u32 *__restrict__ in, u64 n, u64 *__restrict__ out,
+                                                       u64 *__restrict__ status, u32 *__restrict__ ticket,
+                                                       u64 *__restrict__ total, u32 *__restrict__ err)
+{
+    __shared__ u32 s_tile;
+    __shared__ u64 s_warp[SCAN_THREADS / 32];
+    __shared__ u64 s_exclusive;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const u32 tile = s_tile;
+    const u64 base = (u64)tile * SCAN_TILE + (u64)threadIdx.x * SCAN_ITEMS;
+    u32 v[SCAN_ITEMS];
+    u64 local = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        v[k] = (base + k < n) ? in[base + k] : 0u;
+        local += v[k];
+    }
+    // block-wide exclusive scan of the per-thread sums
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u64 x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        u64 y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        u64 w = (lane < SCAN_THREADS / 32) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < SCAN_THREADS / 32; o <<= 1) {
+            u64 y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < SCAN_THREADS / 32) s_warp[lane] = w;
+    }
+    __syncthreads();
+    const u64 block_total = s_warp[SCAN_THREADS / 32 - 1];
+    u64 thread_excl = x - local + (warp ? s_warp[warp - 1] : 0);
+
+    if (threadIdx.x == 0) {
+        u64 excl = 0;
+        if (tile == 0) {
+            st_release(status, ST_PREFIX | block_total);
+        } else {
+            st_release(status + tile, ST_AGG | block_total);
+            long long p = (long long)tile - 1;
+            u32 spins = 0;
+            while (p >= 0) {
+                u64 w = ld_acquire(status + p);
+                if ((w >> 62) == 0) {
+                    if (++spins > SCAN_SPIN_LIMIT) {
+                        atomicOr(err, DEVERR_SCAN_TIMEOUT);
+                        break;
+                    }
+                    continue;
+                }
+                excl += w & ST_VALUE;
+                if ((w >> 62) == 2) break;
+                p--;
+            }
+            st_release(status + tile, ST_PREFIX | (excl + block_total));
+        }
+        s_exclusive = excl;
+        if ((u64)(tile + 1) * SCAN_TILE >= n) *total = excl + block_total;
+    }
+    __syncthreads();
+    u64 run = s_exclusive + thread_excl;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+}
+
+// ---------------------------------------------------------------- generate
+// Each thread owns one position of the level; its moves go to
+// [offs[i], offs[i] + counts[i]) of the next level as (parent i, move).
+constexpr int GEN_THREADS = 128;
+constexpr int GEN_CAP = 8192;  // moves staged per CTA (6 B each = 48 KB)
+
+struct SmemSink {
+    uint16_t *mv;
+    u32 *pi;
+    u32 parent;
+    int n;
+    __device__ __forceinline__ void put(uint16_t m)
+    {
+        mv[n] = m;
+        pi[n] = parent;
+        n++;
+    }
+};
+struct GlobalSink {
+    uint16_t *mv;
+    u32 *pi;
+    u32 parent;
+    u64 n;
+    __device__ __forceinline__ void put(uint16_t m)
+    {
+        mv[n] = m;
+        pi[n] = parent;
+        n++;
+    }
+};
+
+template <int C>
+__global__ void __launch_bounds__(GEN_THREADS) k_generate(const Board *__restrict__ boards,
+                                                          const uint8_t *__restrict__ states,
+                                                          const u64 *__restrict__ offs, const u64 *__restrict__ total,
+                                                          u64 n, uint16_t *__restrict__ out_mv,
+                                                          u32 *__restrict__ out_pi)
+{
+    __shared__ uint16_t s_mv[GEN_CAP];
+    __shared__ u32 s_pi[GEN_CAP];
+    const u64 first = (u64)blockIdx.x * GEN_THREADS;
+    const u64 last = min(first + GEN_THREADS, n);  // exclusive
+    const u64 tile_begin = offs[first];
+    const u64 tile_end = (last < n) ? offs[last] : *total;
+    const u64 i = first + threadIdx.x;
+    const bool staged = (tile_end - tile_begin) <= (u64)GEN_CAP;
+    if (i < n) {
+        Board b = load_board(boards + i);
+        u32 st = states[i];
+        if (staged) {
+            SmemSink s{s_mv, s_pi, (u32)i, (int)(offs[i] - tile_begin)};
+            gen_moves<C>(b, st, s);
+        } else {
+            GlobalSink s{out_mv, out_pi, (u32)i, offs[i]};
+            gen_moves<C>(b, st, s);
+        }
+    }
+    if (!staged) return;
+    __syncthreads();
+    const int cnt = (int)(tile_end - tile_begin);
+    for (int k = threadIdx.x; k < cnt; k += GEN_THREADS) {
+        out_mv[tile_begin + k] = s_mv[k];
+        out_pi[tile_begin + k] = s_pi[k];
+    }
+}
+
+// ---------------------------------------------------------------- leaves
+// One-ply leaf: the move count of each edge's child (perft 1 of the child).
+template <int C>
+__global__ void __launch_bounds__(256) k_leaf1(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                                               const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves, u64 n,
+                                               unsigned long long *__restrict__ counter)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    u32 cnt = 0;
+    if (i < n) {
+        u32 p = pidx[i];
+        Board b = load_board(pboards + p);
+        u32 st = pstates[p];
+        make_move<C>(b, st, moves[i]);
+        cnt = count_moves<1 - C, false>(b, st);
+    }
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(counter, (unsigned long long)cnt);
+}
+
+// Fused two-ply leaf: perft 2 of each edge's child, summed.
+// counter[0] += leaf nodes, counter[1] += positions counted (move-count calls).
+template <int C, bool STRICT>
+__global__ void __launch_bounds__(256) k_leaf2(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                                               const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves, u64 n,
+                                               unsigned long long *__restrict__ counter)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    u32 total = 0, counted = 0;
+    if (i < n) {
+        u32 p = pidx[i];
+        Board b = load_board(pboards + p);
+        u32 st = pstates[p];
+        make_move<C>(b, st, moves[i]);
+        uint16_t mv[MAX_MOVES];
+        ArraySink sink{mv, 0};
+        gen_moves<1 - C>(b, st, sink);
+        for (int k = 0; k < sink.n; k++) {
+            Board g = b;
+            u32 gs = st;
+            make_move<1 - C>(g, gs, mv[k]);
+            total += count_moves<C, STRICT>(g, gs);
+        }
+        counted = sink.n;
+    }
+    total = __reduce_add_sync(0xffffffffu, total);
+    counted = __reduce_add_sync(0xffffffffu, counted);
+    if ((threadIdx.x & 31) == 0 && counted) {
+        atomicAdd(counter, (unsigned long long)total);
+        atomicAdd(counter + 1, (unsigned long long)counted);
+    }
+}
+
+}  // namespace pb

@@ -1,0 +1,136 @@
+// perft_cli.cpp - the perft_gpu command line on top of the C ABI.
+//
+//   perft_gpu <fen> <depth> [<launchdepth>] [-nott] [-dtt <MB>] [-htt <MB>] [-ld <N>] [-cpu] [-strict]
+//
+// Same surface and output as the reference program (perft.cu:13-186):
+// flags may appear anywhere, a third positional argument is the launch depth,
+// no arguments runs the initial position to depth 10, and every depth prints
+//   "\nPerft(%02d): <count>, time: <s> seconds, nps: <n>\n"
+// (launcher.cu:732-735).  -strict is new: it counts the two cases where the
+// reference's move counting merges two moves (see include/perft_b200.h).
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/perft_b200.h"
+
+
+// Decimal text of a 128-bit value by repeated division by 10^9 in 32-bit limbs.
+static std::string u128_text(pb_u128 v)
+{
+    if (v.hi == 0) return std::to_string((unsigned long long)v.lo);
+    uint32_t limb[4] = {(uint32_t)v.lo, (uint32_t)(v.lo >> 32), (uint32_t)v.hi, (uint32_t)(v.hi >> 32)};
+    std::vector<uint32_t> groups;
+    while (limb[0] | limb[1] | limb[2] | limb[3]) {
+        uint64_t rem = 0;
+        for (int i = 3; i >= 0; i--) {
+            uint64_t cur = (rem << 32) | limb[i];
+            limb[i] = (uint32_t)(cur / 1000000000ULL);
+            rem = cur % 1000000000ULL;
+        }
+        groups.push_back((uint32_t)rem);
+    }
+    std::string s = std::to_string(groups.back());
+    char buf[16];
+    for (int i = (int)groups.size() - 2; i >= 0; i--) {
+        snprintf(buf, sizeof(buf), "%09u", groups[i]);
+        s += buf;
+    }
+    return s;
+}
+
+static double u128_double(pb_u128 v) { return (double)v.hi * 18446744073709551616.0 + (double)v.lo; }
+
+static void print_depth(int d, pb_u128 v, double secs)
+{
+    printf("\nPerft(%02d): %s, time: %g seconds", d, u128_text(v).c_str(), secs);
+    if (secs > 0) printf(", nps: %llu", (unsigned long long)(u128_double(v) / secs));
+    printf("\n");
+    fflush(stdout);
+}
+
+int main(int argc, char **argv)
+{
+    bool cpu = false;
+    pb_opts opts;
+    pb_default_opts(&opts);
+    std::vector<std::string> pos;
+    for (int i = 1; i < argc; i++) {
+        std::string a = argv[i];
+        if (a == "-cpu") cpu = true;
+        else if (a == "-nott") opts.use_tt = 0;
+        else if (a == "-strict") opts.strict = 1;
+        else if (a == "-ld" && i + 1 < argc) opts.launch_depth = atoi(argv[++i]);
+        else if (a == "-dtt" && i + 1 < argc) opts.device_tt_mb = atoi(argv[++i]);
+        else if (a == "-htt" && i + 1 < argc) opts.host_tt_mb = atoi(argv[++i]);
+        else pos.push_back(a);
+    }
+    std::string fen = "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1";
+    int max_depth = 10;
+    if (pos.size() >= 2) {
+        if (pos[0].size() > 5) fen = pos[0];
+        max_depth = atoi(pos[1].c_str());
+        if (pos.size() >= 3 && opts.launch_depth == 0) opts.launch_depth = atoi(pos[2].c_str());
+    } else {
+        printf("\nUsage: perft_gpu <fen> <depth> [<launchdepth>] [-nott] [-dtt <MB>] [-htt <MB>] [-ld <N>] [-cpu] [-strict]\n");
+        printf("\nAs no parameters were provided... running default test\n");
+    }
+    pb_pos root;
+    if (pb_parse_fen(fen.c_str(), &root) != PB_OK) {
+        fprintf(stderr, "invalid FEN: %s\n", fen.c_str());
+        return 1;
+    }
+    if (max_depth < 1 || max_depth > 30) {
+        fprintf(stderr, "depth must be 1..30\n");
+        return 1;
+    }
+    pb_ctx *ctx = nullptr;
+    if (cpu) {
+        printf("CPU mode\n");
+        fflush(stdout);
+        opts.use_tt = 0;
+        if (pb_create(-1, &opts, &ctx) != PB_OK) return 1;
+        for (int d = 1; d <= max_depth; d++) {
+            pb_u128 v;
+            double secs = 0;
+            int rc = pb_perft_launch(ctx, &root, d, &v, &secs);
+            if (rc != PB_OK) {
+                fprintf(stderr, "error: %s\n", pb_last_error(ctx));
+                return 1;
+            }
+            print_depth(d, v, secs);
+        }
+        pb_destroy(ctx);
+        return 0;
+    }
+    int ngpu = pb_device_count();
+    printf("No of GPUs detected: %d\n", ngpu);
+    if (ngpu == 0) {
+        printf("No CUDA GPUs found. Exiting.\n");
+        return 1;
+    }
+    opts.verbose = 1;
+    int rc = pb_create(0, &opts, &ctx);
+    if (rc != PB_OK) {
+        fprintf(stderr, "init failed (%d)\n", rc);
+        return 1;
+    }
+    printf("Launch depth: %d\n", pb_choose_launch_depth(ctx, &root));
+    fflush(stdout);
+    for (int d = 1; d <= max_depth; d++) {
+        pb_u128 v;
+        double secs = 0;
+        rc = pb_perft_launch(ctx, &root, d, &v, &secs);
+        if (rc != PB_OK) {
+            fprintf(stderr, "error: %s\n", pb_last_error(ctx));
+            pb_destroy(ctx);
+            return 1;
+        }
+        print_depth(d, v, secs);
+    }
+    pb_destroy(ctx);
+    return 0;
+}

@@ -1,0 +1,143 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle, the
+reference-generated fixtures and the reference README's known totals."""
+import os
+import subprocess
+
+import pytest
+
+import perft_gpu_2026_b200 as pg
+
+pytestmark = pytest.mark.gpu
+
+START = pg.START_FEN
+KIWIPETE = "r3k2r/p1ppqpb1/bn2pnp1/3PN3/1p2P3/2N2Q1p/PPPBBPPP/R3K2R w KQkq -"  # README.md:32
+
+
+def test_scan_matches_torch(gpu_engine):
+    import torch
+
+    g = torch.Generator().manual_seed(0)
+    for n in (1, 31, 2047, 2048, 2049, 100_003, 5_000_000):
+        x = torch.randint(0, 219, (n,), generator=g, dtype=torch.int64)
+        d_in = x.to(torch.int32).cuda()
+        d_out = torch.empty(n, dtype=torch.int64, device="cuda")
+        d_tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+        gpu_engine.dev_scan(d_in.data_ptr(), n, d_out.data_ptr(), d_tot.data_ptr())
+        torch.cuda.synchronize()
+        excl = torch.cumsum(x, 0) - x
+        assert torch.equal(d_out.cpu(), excl), n
+        assert int(d_tot.item()) == int(x.sum()), n
+
+
+def test_gpu_matches_reference_fixtures(gpu_engine, golden):
+    bad = []
+    for case in golden:
+        p = pg.parse_fen(case["fen"])
+        for d, want in enumerate(case["counts"], start=1):
+            got = gpu_engine.perft_position(p, d)
+            if got != want:
+                bad.append((case["name"], d, got, want))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("strict", [False, True])
+def test_gpu_matches_oracle_on_playouts(oracle, strict):
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30, strict=strict)
+    for seed in range(40):
+        p, _, _ = pg.random_playout(50_000 + seed, 6 + (seed * 17) % 60)
+        if pg.count_moves(p, True) == 0:
+            continue
+        fen = pg.to_fen(p)
+        for d in (3, 4):
+            assert eng.perft_position(p, d) == oracle.perft(fen, d, strict), (fen, d)
+    eng.close()
+
+
+def test_strict_mode_counts_merged_moves():
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30, strict=True)
+    p = pg.parse_fen("2n4k/1P1P4/8/8/8/8/8/4K3 w - - 0 1")
+    assert [eng.perft_position(p, d) for d in (1, 2, 3, 4)][:1] == [21]
+    comp = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30)
+    assert comp.perft_position(p, 1) == 17
+    eng.close()
+    comp.close()
+
+
+def test_readme_known_totals(gpu_engine):
+    # README.md:51-52 and :92 (RTX PRO 6000 / GB10 tables)
+    assert gpu_engine.perft_position(pg.parse_fen(START), 8) == 84_998_978_956
+    assert gpu_engine.perft_position(pg.parse_fen(KIWIPETE), 7) == 374_190_009_323
+
+
+def test_readme_startpos_perft9(gpu_engine):
+    # README.md:51: 2,439,530,234,167
+    assert gpu_engine.perft_position(pg.parse_fen(START), 9) == 2_439_530_234_167
+
+
+def test_config1_small_workload(gpu_engine, golden, oracle):
+    p = pg.config_position(8, 0)
+    want = {c["name"]: c for c in golden}["cfg_8ply_seed0"]["counts"]
+    assert [gpu_engine.perft_position(p, d) for d in range(1, 6)] == want
+    assert gpu_engine.perft_position(p, 5) == oracle.perft(pg.to_fen(p), 5)
+
+
+def test_bench_workload_divide_consistency(gpu_engine):
+    """perft 7 of the bench position equals the sum of perft 6 over its
+    children and the launch-depth split (size-independent properties)."""
+    p = pg.config_position(4, 1)
+    whole = gpu_engine.perft_position(p, 7)
+    parts = sum(gpu_engine.perft_position(pg.make_move(p, m), 6) for m in pg.generate_moves(p))
+    assert whole == parts
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30, launch_depth=5)
+    split, _ = eng.perft_launch(p, 7)
+    eng.close()
+    assert whole == split
+
+
+def test_bench_position_perft6_vs_oracle(gpu_engine, oracle):
+    p = pg.config_position(4, 1)
+    fen = pg.to_fen(p)
+    assert gpu_engine.perft_position(p, 6) == oracle.perft(fen, 6)
+
+
+def test_small_arena_splits_the_root():
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 20)
+    p = pg.parse_fen(START)
+    assert eng.perft_position(p, 6) == 119_060_324
+    eng.close()
+
+
+def test_perft_launch_host_recursion():
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30, launch_depth=4)
+    res = eng.perft(START, 6)
+    assert [r for r, _ in res] == [20, 400, 8902, 197281, 4865609, 119060324]
+    eng.close()
+
+
+def test_batch_matches_oracle(oracle):
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30)
+    roots = pg.uneven_roots(48, 6, 40, seed=2)
+    got = eng.perft_batch(roots, [4] * len(roots))
+    want = [oracle.perft(pg.to_fen(r), 4) for r in roots]
+    assert got == want
+    eng.close()
+
+
+def test_stats_and_timing(gpu_engine):
+    p = pg.config_position(4, 1)
+    gpu_engine.set_timing(True)
+    n = gpu_engine.perft_position(p, 6)
+    st = gpu_engine.last_stats()
+    gpu_engine.set_timing(False)
+    assert st.nodes == n
+    assert st.leaf_ms > 0 and st.device_ms >= st.leaf_ms
+    assert st.leaf_positions > st.leaf_edges > 0
+    assert st.kernels == 3 * st.levels + 1
+
+
+def test_cli_gpu_output():
+    cli = os.path.join(os.path.dirname(pg.__file__), "perft_gpu")
+    out = subprocess.run([cli, KIWIPETE, "5", "-nott"], capture_output=True, text=True, check=True).stdout
+    lines = [l.split(",")[0] for l in out.splitlines() if l.startswith("Perft(")]
+    assert lines == ["Perft(01): 48", "Perft(02): 2039", "Perft(03): 97862", "Perft(04): 4085603",
+                     "Perft(05): 193690690"]

@@ -1,0 +1,113 @@
+"""Host side of the engine (no GPU): the C ABI's chess core, FEN handling and
+the workload generator, checked against the oracle and the fixtures."""
+import ctypes
+
+import pytest
+
+import perft_gpu_2026_b200 as pg
+
+
+def test_host_perft_matches_fixtures(golden):
+    eng = pg.Engine(device=-1)
+    bad = []
+    for case in golden:
+        p = pg.parse_fen(case["fen"])
+        for d, want in enumerate(case["counts"], start=1):
+            if want > 30_000_000:
+                continue
+            got = eng.perft_cpu(p, d)
+            if got != want:
+                bad.append((case["name"], d, got, want))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("strict", [False, True])
+def test_host_core_matches_oracle_on_playouts(oracle, strict):
+    eng = pg.Engine(device=-1, strict=strict)
+    for seed in range(120):
+        p, _, _ = pg.random_playout(7000 + seed, 4 + (seed * 13) % 70)
+        fen = pg.to_fen(p)
+        for d in (1, 2, 3):
+            assert eng.perft_cpu(p, d) == oracle.perft(fen, d, strict), (fen, d)
+
+
+def test_generation_matches_strict_count(golden):
+    for case in golden:
+        p = pg.parse_fen(case["fen"])
+        assert len(pg.generate_moves(p)) == pg.count_moves(p, strict=True), case["name"]
+
+
+def test_generated_moves_match_oracle_as_sets(oracle, golden):
+    for case in golden:
+        p = pg.parse_fen(case["fen"])
+        mine = sorted(pg.move_uci(m) for m in pg.generate_moves(p))
+        ref = sorted(pg.move_uci(m) for m in oracle.moves(case["fen"]))
+        assert mine == ref, case["name"]
+
+
+def test_fen_round_trip(golden):
+    for case in golden:
+        p = pg.parse_fen(case["fen"])
+        q = pg.parse_fen(pg.to_fen(p))
+        assert p.key() == q.key(), case["name"]
+
+
+@pytest.mark.parametrize("fen", [
+    "8/8/8/8/8/8/8/8 w - - 0 1",            # no kings
+    "4k3/8/8/8/8/8/8/4KK2 w - - 0 1",       # two white kings
+    "4k3/4K3/8/8/8/8/8/8 w - - 0 1",        # adjacent kings
+    "4k3/8/8/8/8/8/8/P3K3 w - - 0 1",       # pawn on the first rank
+    "4k3/8/8/8/8/8/8/4R2K w - - 0 1",       # black (not to move) in check
+])
+def test_fen_rejects_impossible_positions(fen):
+    with pytest.raises(pg.PerftError):
+        pg.parse_fen(fen)
+
+
+def test_fen_drops_inconsistent_rights_and_ep():
+    p = pg.parse_fen("4k3/8/8/8/8/8/8/4K3 w KQkq e6 0 1")
+    assert p.state == 0
+    p = pg.parse_fen("4k3/8/8/3Pp3/8/8/8/4K3 w - e6 0 1")
+    assert p.state >> 4 == 5
+
+
+def test_playout_generator_matches_oracle(oracle):
+    for seed in range(40):
+        plies = 1 + seed % 50
+        p, n, st = pg.random_playout(seed, plies)
+        ofen, on, ost = oracle.playout_fen(seed, plies)
+        assert n == on and st == ost
+        q = pg.parse_fen(ofen)
+        # the oracle (like the reference -cpu path) records an en-passant file
+        # after every double push; the engine only when a capture can follow
+        assert p.key()[:4] == q.key()[:4] and p.color == q.color
+        assert p.state & 15 == q.state & 15
+        if p.state >> 4:
+            assert p.state >> 4 == q.state >> 4
+
+
+def test_config_positions_are_stable(golden):
+    byname = {c["name"]: c for c in golden}
+    for name in ("cfg_8ply_seed0", "cfg_4ply_seed1", "cfg_2ply_seed4"):
+        c = byname[name]
+        p = pg.config_position(c["plies"], c["seed"])
+        assert pg.to_fen(p) == c["fen"]
+
+
+def test_uneven_roots_have_moves():
+    roots = pg.uneven_roots(64, 6, 40, seed=2)
+    assert len(roots) == 64
+    assert all(pg.count_moves(r, True) > 0 for r in roots)
+    again = pg.uneven_roots(64, 6, 40, seed=2)
+    assert [r.key() for r in roots] == [r.key() for r in again]
+
+
+def test_cpu_cli_output_format():
+    import os
+    import subprocess
+    cli = os.path.join(os.path.dirname(pg.__file__), "perft_gpu")
+    out = subprocess.run([cli, pg.START_FEN, "4", "-cpu"], capture_output=True, text=True, check=True).stdout
+    lines = [l for l in out.splitlines() if l.startswith("Perft(")]
+    assert [l.split(",")[0] for l in lines] == ["Perft(01): 20", "Perft(02): 400", "Perft(03): 8902",
+                                                 "Perft(04): 197281"]
+    assert all(" seconds" in l for l in lines)
