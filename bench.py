@@ -197,6 +197,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--depth", type=int, default=WORKLOAD["depth"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--leaf-kernel", type=int, default=0, help="1 = edge per thread, 2 = cooperative (0 = engine default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -222,6 +223,8 @@ def main():
     depth = args.depth
     eng = pg.Engine(device=local, use_tt=False)
     eng.set_timing(True)
+    if args.leaf_kernel:
+        eng.set_tuning(leaf_kernel=args.leaf_kernel)
 
     # shard: depth-2 subtrees round-robin over ranks (one rank: the whole root)
     if world > 1:

@@ -143,6 +143,20 @@ typedef struct {
     uint64_t d2h_bytes;        /* device-to-host bytes copied */
 } pb_stats;
 
+/* Launch parameters of the GPU path (no reference counterpart: the
+ * reference fixes them at compile time, switches.h:8-24, perft_kernels.cu:74).
+ * Zero fields keep the current value.  leaf_kernel: 1 = one edge per thread,
+ * 2 = cooperative (grandchildren spread over the CTA);
+ * leaf_blocks_per_sm: persistent grid of the cooperative leaf. */
+typedef struct {
+    int leaf_kernel;
+    int leaf_blocks_per_sm;
+    int reserved[6];
+} pb_tuning;
+
+int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t);
+int pb_get_tuning(const pb_ctx *ctx, pb_tuning *t);
+
 /* Turns per-call event timing on or off (off by default). */
 int pb_set_timing(pb_ctx *ctx, int enable);
 int pb_last_stats(const pb_ctx *ctx, pb_stats *out);

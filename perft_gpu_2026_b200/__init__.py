@@ -19,7 +19,7 @@ from dataclasses import dataclass
 from typing import List, Optional, Sequence, Tuple
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libperftb200.so")
+LIB_PATH = os.environ.get("PERFT_B200_LIB") or os.path.join(_HERE, "libperftb200.so")
 
 START_FEN = "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1"
 
@@ -82,6 +82,13 @@ class Stats(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    """pb_tuning: launch parameters (zero = keep current)."""
+
+    _fields_ = [("leaf_kernel", ctypes.c_int), ("leaf_blocks_per_sm", ctypes.c_int),
+                ("reserved", ctypes.c_int * 6)]
+
+
 class PerftError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"perft engine error {code}: {msg}")
@@ -113,6 +120,8 @@ def _load() -> ctypes.CDLL:
         "pb_device_count": (ctypes.c_int, []),
         "pb_choose_launch_depth": (ctypes.c_int, [ctypes.c_void_p, P(Pos)]),
         "pb_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+        "pb_set_tuning": (ctypes.c_int, [ctypes.c_void_p, P(Tuning)]),
+        "pb_get_tuning": (ctypes.c_int, [ctypes.c_void_p, P(Tuning)]),
         "pb_last_stats": (ctypes.c_int, [ctypes.c_void_p, P(Stats)]),
         "pb_dev_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
     }
@@ -315,6 +324,17 @@ class Engine:
 
     def set_timing(self, enable: bool = True) -> None:
         self._check(lib.pb_set_timing(self._h, int(enable)))
+
+    def set_tuning(self, leaf_kernel: int = 0, leaf_blocks_per_sm: int = 0) -> None:
+        t = Tuning()
+        t.leaf_kernel = leaf_kernel
+        t.leaf_blocks_per_sm = leaf_blocks_per_sm
+        self._check(lib.pb_set_tuning(self._h, ctypes.byref(t)))
+
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        self._check(lib.pb_get_tuning(self._h, ctypes.byref(t)))
+        return t
 
     def last_stats(self) -> Stats:
         st = Stats()

@@ -92,12 +92,24 @@ PB_HD int popc(u64 x)
     return __builtin_popcountll(x);
 #endif
 }
+// Index of the lowest set bit (x != 0).  On the GPU this is a population
+// count of the bits below it: POPC issues on the XU pipe, which leaves the
+// ALU pipe (the leaf kernel's bottleneck) free.
 PB_HD int lsb(u64 x)
 {
 #ifdef __CUDA_ARCH__
-    return __ffsll((long long)x) - 1;
+    return __popcll((x - 1) & ~x);
 #else
     return __builtin_ctzll(x);
+#endif
+}
+// Index of a single set bit.
+PB_HD int bit_index(u64 single)
+{
+#ifdef __CUDA_ARCH__
+    return __popcll(single - 1);
+#else
+    return __builtin_ctzll(single);
 #endif
 }
 PB_HD bool more_than_one(u64 x) { return (x & (x - 1)) != 0; }
@@ -127,10 +139,12 @@ PB_HD u64 ldg64(const u64 *p) { return *p; }
 PB_HD u64 magic_lookup(const Magic *e, u64 occ)
 {
 #ifdef __CUDA_ARCH__
+    // bits <= 12, so the index lies in the high word of the product: one
+    // 32-bit shift by (shift - 32) instead of a 64-bit variable shift
     ulonglong2 mm = __ldg(reinterpret_cast<const ulonglong2 *>(e));
     uint2 os = __ldg(reinterpret_cast<const uint2 *>(&e->offset));
-    u64 idx = ((occ & mm.x) * mm.y) >> os.y;
-    return __ldg(&g_attacks[os.x + (u32)idx]);
+    u32 hi = (u32)(((occ & mm.x) * mm.y) >> 32);
+    return __ldg(&g_attacks[os.x + (hi >> (os.y - 32))]);
 #else
     u64 idx = ((occ & e->mask) * e->magic) >> e->shift;
     return h_attacks[e->offset + (u32)idx];
@@ -215,7 +229,7 @@ template <int C> PB_HD u64 enemy_attacks(const Sets &s, u64 my_king)
     u64 ep = s.pawns & s.them;
     u64 a = cap_west<1 - C>(ep) | cap_east<1 - C>(ep);
     a |= knights_bulk(s.knights & s.them);
-    a |= king_att(lsb(s.kings & s.them));
+    a |= king_att(bit_index(s.kings & s.them));
     u64 occ = s.occ ^ my_king;
     u64 b = s.bq & s.them;
     while (b) {
@@ -244,7 +258,7 @@ PB_HD u32 count_evasions(const Sets &s, u32 state, u64 pinned, u64 threat, int k
     u32 n = popc(king_att(ksq) & ~(threat | s.us));
     if (more_than_one(checkers)) return n;
 
-    u64 safe = checkers | between(ksq, lsb(checkers));
+    u64 safe = checkers | between(ksq, bit_index(checkers));
     u64 mine = s.us & ~pinned;
     u64 empty = ~s.occ;
     u64 pawns = s.pawns & mine;
@@ -289,7 +303,7 @@ PB_HD u32 count_moves(const Board &b, u32 state)
 {
     Sets s = derive<C>(b);
     u64 my_king = s.kings & s.us;
-    int ksq = lsb(my_king);
+    int ksq = bit_index(my_king);
     u64 eb = s.bq & s.them, er = s.rq & s.them;
     u64 pinned = pinned_set(ksq, eb, er, s.occ);
     u64 threat = enemy_attacks<C>(s, my_king);
@@ -361,21 +375,18 @@ PB_HD u32 count_moves(const Board &b, u32 state)
         n += popc(knight_att(lsb(kn)) & ~s.us);
         kn &= kn - 1;
     }
-    u64 bs = s.bq & s.us;
-    while (bs) {
-        int sq = lsb(bs);
-        u64 m = bishop_att(sq, s.occ) & ~s.us;
-        if (pinned & (1ULL << sq)) m &= line_through(sq, ksq);
-        n += popc(m);
-        bs &= bs - 1;
-    }
-    u64 rs = s.rq & s.us;
-    while (rs) {
-        int sq = lsb(rs);
-        u64 m = rook_att(sq, s.occ) & ~s.us;
-        if (pinned & (1ULL << sq)) m &= line_through(sq, ksq);
-        n += popc(m);
-        rs &= rs - 1;
+    for (u64 bs = s.bq & s.us & ~pinned; bs; bs &= bs - 1) n += popc(bishop_att(lsb(bs), s.occ) & ~s.us);
+    for (u64 rs = s.rq & s.us & ~pinned; rs; rs &= rs - 1) n += popc(rook_att(lsb(rs), s.occ) & ~s.us);
+    if (pinned & (s.bq | s.rq)) {
+        // a pinned slider moves only along the line through its king
+        for (u64 bs = s.bq & s.us & pinned; bs; bs &= bs - 1) {
+            int sq = lsb(bs);
+            n += popc(bishop_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
+        }
+        for (u64 rs = s.rq & s.us & pinned; rs; rs &= rs - 1) {
+            int sq = lsb(rs);
+            n += popc(rook_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
+        }
     }
     return n;
 }
@@ -419,7 +430,7 @@ PB_HD void gen_evasions(const Sets &s, u32 state, u64 pinned, u64 threat, int ks
     emit_targets(sink, ksq, king_att(ksq) & ~(threat | s.us));
     if (more_than_one(checkers)) return;
 
-    u64 safe = checkers | between(ksq, lsb(checkers));
+    u64 safe = checkers | between(ksq, bit_index(checkers));
     u64 mine = s.us & ~pinned;
     u64 empty = ~s.occ;
     u64 ept = ep_target<C>(state);
@@ -474,7 +485,7 @@ template <int C, class Sink> PB_HD void gen_moves(const Board &b, u32 state, Sin
 {
     Sets s = derive<C>(b);
     u64 my_king = s.kings & s.us;
-    int ksq = lsb(my_king);
+    int ksq = bit_index(my_king);
     u64 eb = s.bq & s.them, er = s.rq & s.them;
     u64 pinned = pinned_set(ksq, eb, er, s.occ);
     u64 threat = enemy_attacks<C>(s, my_king);

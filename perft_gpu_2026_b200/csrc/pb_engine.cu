@@ -45,6 +45,10 @@ struct pb_ctx {
     u64 *h_pinned = nullptr;  // pinned host words for readbacks
     int launch_depth = 0;
     bool timing = false;
+    pb_tuning tuning{1, 0, {0, 0, 0, 0, 0, 0}};
+    int num_sms = 0;
+    uint16_t *spill = nullptr;  // cooperative-leaf spill area (device)
+    size_t spill_blocks = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // call start, leaf start, leaf end, call end
     pb_stats stats{};
     HostTT htt;
@@ -141,6 +145,36 @@ struct Arena {
 inline unsigned grid_for(u64 n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 enum { BFS_OK = 0, BFS_TOO_BIG = 1 };
+
+template <int C, bool S>
+int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi, const uint16_t *mv, u64 n)
+{
+    cudaStream_t s = ctx->stream;
+    if (ctx->tuning.leaf_kernel == 1) {
+        k_leaf2<C, S><<<grid_for(n, PB_LEAF_THREADS), PB_LEAF_THREADS, 0, s>>>(b, st, pi, mv, n, ctx->d_counter);
+        PB_CUDA(cudaGetLastError());
+        return PB_OK;
+    }
+    u64 nchunks = (n + LEAF_T - 1) / LEAF_T;
+    int per_sm = ctx->tuning.leaf_blocks_per_sm;
+    if (per_sm <= 0) {
+        PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf2_coop<C, S>, LEAF_T, 0));
+        if (per_sm <= 0) per_sm = 1;
+    }
+    u64 grid = std::min<u64>(nchunks, (u64)ctx->num_sms * per_sm);
+    if (grid > ctx->spill_blocks) return fail(ctx, PB_ERR_NOMEM, "leaf spill area too small");
+    k_leaf2_coop<C, S><<<(unsigned)grid, LEAF_T, 0, s>>>(b, st, pi, mv, n, ctx->spill, ctx->d_counter);
+    PB_CUDA(cudaGetLastError());
+    return PB_OK;
+}
+
+int launch_leaf(pb_ctx *ctx, int c, bool strict, const Board *b, const uint8_t *st, const u32 *pi,
+                const uint16_t *mv, u64 n)
+{
+    if (c == WHITE) return strict ? launch_leaf_t<WHITE, true>(ctx, b, st, pi, mv, n)
+                                  : launch_leaf_t<WHITE, false>(ctx, b, st, pi, mv, n);
+    return strict ? launch_leaf_t<BLACK, true>(ctx, b, st, pi, mv, n) : launch_leaf_t<BLACK, false>(ctx, b, st, pi, mv, n);
+}
 
 // One GPU breadth-first perft; status BFS_TOO_BIG when a level would not fit.
 int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth, u64 *out, int *bfs_status)
@@ -239,19 +273,9 @@ int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth,
         c = 1 - c;
     }
     PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(unsigned long long), s));
-    unsigned g = grid_for(n, 256);
     if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[1], s));
-    if (c == WHITE) {
-        if (strict)
-            k_leaf2<WHITE, true><<<g, 256, 0, s>>>(cur_b, cur_s, epi, emv, n, ctx->d_counter);
-        else
-            k_leaf2<WHITE, false><<<g, 256, 0, s>>>(cur_b, cur_s, epi, emv, n, ctx->d_counter);
-    } else {
-        if (strict)
-            k_leaf2<BLACK, true><<<g, 256, 0, s>>>(cur_b, cur_s, epi, emv, n, ctx->d_counter);
-        else
-            k_leaf2<BLACK, false><<<g, 256, 0, s>>>(cur_b, cur_s, epi, emv, n, ctx->d_counter);
-    }
+    int rc = launch_leaf(ctx, c, strict, cur_b, cur_s, epi, emv, n);
+    if (rc != PB_OK) return rc;
     PB_CUDA(cudaGetLastError());
     if (ctx->timing) {
         PB_CUDA(cudaEventRecord(ctx->ev[2], s));
@@ -414,7 +438,10 @@ int pb_create(int device, const pb_opts *opts, pb_ctx **out)
             ctx->d_err = reinterpret_cast<u32 *>(small + 64);
             ctx->d_ticket = reinterpret_cast<u32 *>(small + 128);
             ctx->d_total = reinterpret_cast<u64 *>(small + 192);
-            if ((e = cudaMallocHost(&ctx->h_pinned, 64)) != cudaSuccess) { rc = cuda_fail(ctx, e, "pinned"); break; }
+            if ((e = cudaMallocHost(&ctx->h_pinned, 4096)) != cudaSuccess) { rc = cuda_fail(ctx, e, "pinned"); break; }
+            if ((e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) { rc = cuda_fail(ctx, e, "sm count"); break; }
+            ctx->spill_blocks = (size_t)ctx->num_sms * 8;
+            if ((e = cudaMalloc(&ctx->spill, ctx->spill_blocks * LEAF_T * LEAF_OVF * sizeof(uint16_t))) != cudaSuccess) { rc = cuda_fail(ctx, e, "spill"); break; }
             size_t freeb = 0, totalb = 0;
             cudaMemGetInfo(&freeb, &totalb);
             size_t want = ctx->opts.arena_bytes;
@@ -453,6 +480,7 @@ void pb_destroy(pb_ctx *ctx)
             if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
         if (ctx->arena) cudaFree(ctx->arena);
         if (ctx->d_counter) cudaFree(ctx->d_counter);
+        if (ctx->spill) cudaFree(ctx->spill);
         if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
     }
@@ -526,6 +554,27 @@ int pb_set_timing(pb_ctx *ctx, int enable)
     if (enable && !ctx->ev[0])
         for (int i = 0; i < 4; i++) PB_CUDA(cudaEventCreate(&ctx->ev[i]));
     ctx->timing = enable != 0;
+    return PB_OK;
+}
+
+int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
+{
+    if (!ctx || !t) return PB_ERR_ARG;
+    if (t->leaf_kernel) {
+        if (t->leaf_kernel < 1 || t->leaf_kernel > 2) return PB_ERR_ARG;
+        ctx->tuning.leaf_kernel = t->leaf_kernel;
+    }
+    if (t->leaf_blocks_per_sm) {
+        if (t->leaf_blocks_per_sm < 0 || t->leaf_blocks_per_sm > 8) return PB_ERR_ARG;
+        ctx->tuning.leaf_blocks_per_sm = t->leaf_blocks_per_sm;
+    }
+    return PB_OK;
+}
+
+int pb_get_tuning(const pb_ctx *ctx, pb_tuning *t)
+{
+    if (!ctx || !t) return PB_ERR_ARG;
+    *t = ctx->tuning;
     return PB_OK;
 }
 

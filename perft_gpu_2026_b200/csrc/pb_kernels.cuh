@@ -251,8 +251,17 @@ __global__ void __launch_bounds__(256) k_leaf1(const Board *__restrict__ pboards
 
 // Fused two-ply leaf: perft 2 of each edge's child, summed.
 // counter[0] += leaf nodes, counter[1] += positions counted (move-count calls).
+// Block size and the minimum resident blocks per SM trade registers against
+// warps in flight; the kernel is ALU-pipe bound, so enough warps must be
+// resident to keep the pipe fed through the table-load latency.
+#ifndef PB_LEAF_THREADS
+#define PB_LEAF_THREADS 256
+#endif
+#ifndef PB_LEAF_MIN_BLOCKS
+#define PB_LEAF_MIN_BLOCKS 4
+#endif
 template <int C, bool STRICT>
-__global__ void __launch_bounds__(256) k_leaf2(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS) k_leaf2(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                                                const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves, u64 n,
                                                unsigned long long *__restrict__ counter)
 {
@@ -279,6 +288,138 @@ __global__ void __launch_bounds__(256) k_leaf2(const Board *__restrict__ pboards
     if ((threadIdx.x & 31) == 0 && counted) {
         atomicAdd(counter, (unsigned long long)total);
         atomicAdd(counter + 1, (unsigned long long)counted);
+    }
+}
+
+}  // namespace pb
+
+namespace pb {
+
+// ---------------------------------------------------------------- cooperative leaf
+// Fused two-ply leaf with the grandchild work spread over the whole CTA.
+//
+// Per chunk of LEAF_T edges:
+//   phase A  thread t makes edge t's move (child X_t in shared memory) and
+//            generates X_t's moves into its column of a shared-memory move
+//            table (moves beyond LEAF_CAP spill to a per-CTA global area);
+//   scan     block-wide exclusive scan of the move counts, and an owner map
+//            item -> t (one byte per item) built from it;
+//   phase B  the chunk's N = sum n_t (child, move) items are dealt round-robin
+//            to the CTA's threads: each item makes the move on X_owner and
+//            counts the grandchild's moves.
+// Adjacent lanes therefore count grandchildren of the same child, so a warp
+// stays converged far better than with one edge per thread, and no thread
+// idles while a neighbour finishes a long move list.
+constexpr int LEAF_T = 256;
+constexpr int LEAF_CAP = 40;                 // moves per child kept in shared memory
+constexpr int LEAF_OVF = MAX_MOVES - LEAF_CAP;  // spill slots per child (global)
+
+struct ColumnSink {
+    uint16_t *col;   // shared: column t of a [LEAF_CAP][LEAF_T] table
+    uint16_t *ovf;   // global spill slots of this child
+    int n;
+    __device__ __forceinline__ void put(uint16_t m)
+    {
+        if (n < LEAF_CAP)
+            col[n * LEAF_T] = m;
+        else
+            ovf[n - LEAF_CAP] = m;
+        n++;
+    }
+};
+
+template <int C, bool STRICT>
+__global__ void __launch_bounds__(LEAF_T, 4) k_leaf2_coop(const Board *__restrict__ pboards,
+                                                          const uint8_t *__restrict__ pstates,
+                                                          const u32 *__restrict__ pidx,
+                                                          const uint16_t *__restrict__ moves, u64 n,
+                                                          uint16_t *__restrict__ spill,
+                                                          unsigned long long *__restrict__ counter)
+{
+    __shared__ Board s_child[LEAF_T];
+    __shared__ uint8_t s_cst[LEAF_T];
+    __shared__ uint16_t s_mv[LEAF_CAP * LEAF_T];
+    __shared__ u32 s_off[LEAF_T + 1];
+    __shared__ uint8_t s_own[LEAF_CAP * LEAF_T];
+    __shared__ u32 s_wsum[LEAF_T / 32];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint16_t *my_spill = spill + ((u64)blockIdx.x * LEAF_T + tid) * LEAF_OVF;
+    u64 total = 0, counted = 0;
+    const u64 nchunks = (n + LEAF_T - 1) / LEAF_T;
+    for (u64 chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+        // ---- phase A: child position and its move list
+        const u64 e = chunk * LEAF_T + tid;
+        int cnt = 0;
+        if (e < n) {
+            u32 p = pidx[e];
+            Board b = load_board(pboards + p);
+            u32 st = pstates[p];
+            make_move<C>(b, st, moves[e]);
+            s_child[tid] = b;
+            s_cst[tid] = (uint8_t)st;
+            ColumnSink sink{s_mv + tid, my_spill, 0};
+            gen_moves<1 - C>(b, st, sink);
+            cnt = sink.n;
+        }
+        // ---- block exclusive scan of cnt
+        u32 x = (u32)cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            u32 y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            u32 w = (lane < LEAF_T / 32) ? s_wsum[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < LEAF_T / 32; o <<= 1) {
+                u32 y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            if (lane < LEAF_T / 32) s_wsum[lane] = w;
+        }
+        __syncthreads();
+        const u32 excl = x - (u32)cnt + (warp ? s_wsum[warp - 1] : 0);
+        s_off[tid] = excl;
+        if (tid == LEAF_T - 1) s_off[LEAF_T] = excl + (u32)cnt;
+        const u32 items = s_wsum[LEAF_T / 32 - 1];
+        counted += (tid == 0) ? items : 0;
+        // ---- phase B in windows of LEAF_CAP * LEAF_T items (owner map size)
+        for (u32 w0 = 0; w0 < items; w0 += LEAF_CAP * LEAF_T) {
+            const u32 w1 = min(items, w0 + (u32)(LEAF_CAP * LEAF_T));
+            // owner map for [w0, w1): thread t marks its items inside the window
+            {
+                u32 a = max(excl, w0), z = min(excl + (u32)cnt, w1);
+                for (u32 k = a; k < z; k++) s_own[k - w0] = (uint8_t)tid;
+            }
+            __syncthreads();
+            for (u32 i = w0 + tid; i < w1; i += LEAF_T) {
+                const int t = s_own[i - w0];
+                const u32 j = i - s_off[t];
+                uint16_t m = (j < (u32)LEAF_CAP)
+                                 ? s_mv[j * LEAF_T + t]
+                                 : spill[((u64)blockIdx.x * LEAF_T + t) * LEAF_OVF + (j - LEAF_CAP)];
+                Board g = s_child[t];
+                u32 gs = s_cst[t];
+                make_move<1 - C>(g, gs, m);
+                total += count_moves<C, STRICT>(g, gs);
+            }
+            __syncthreads();
+        }
+        __syncthreads();  // s_wsum / s_child are rewritten by the next chunk
+    }
+    // ---- one atomic pair per warp
+    unsigned long long t64 = total;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) t64 += __shfl_xor_sync(0xffffffffu, t64, o);
+    unsigned long long c64 = counted;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c64 += __shfl_xor_sync(0xffffffffu, c64, o);
+    if (lane == 0) {
+        if (t64) atomicAdd(counter, t64);
+        if (c64) atomicAdd(counter + 1, c64);
     }
 }
 

@@ -29,7 +29,9 @@ def test_scan_matches_torch(gpu_engine):
         assert int(d_tot.item()) == int(x.sum()), n
 
 
-def test_gpu_matches_reference_fixtures(gpu_engine, golden):
+@pytest.mark.parametrize("leaf_kernel", [1, 2])
+def test_gpu_matches_reference_fixtures(gpu_engine, golden, leaf_kernel):
+    gpu_engine.set_tuning(leaf_kernel=leaf_kernel)
     bad = []
     for case in golden:
         p = pg.parse_fen(case["fen"])
@@ -37,6 +39,7 @@ def test_gpu_matches_reference_fixtures(gpu_engine, golden):
             got = gpu_engine.perft_position(p, d)
             if got != want:
                 bad.append((case["name"], d, got, want))
+    gpu_engine.set_tuning(leaf_kernel=2)
     assert not bad, bad
 
 
@@ -53,20 +56,25 @@ def test_gpu_matches_oracle_on_playouts(oracle, strict):
     eng.close()
 
 
-def test_strict_mode_counts_merged_moves():
+def test_strict_mode_counts_merged_moves(oracle):
     eng = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30, strict=True)
-    p = pg.parse_fen("2n4k/1P1P4/8/8/8/8/8/4K3 w - - 0 1")
-    assert [eng.perft_position(p, d) for d in (1, 2, 3, 4)][:1] == [21]
+    fen = "2n4k/1P1P4/8/8/8/8/8/4K3 w - - 0 1"
+    p = pg.parse_fen(fen)
+    assert eng.perft_position(p, 1) == 21
+    assert [eng.perft_position(p, d) for d in (2, 3, 4, 5)] == [oracle.perft(fen, d, True) for d in (2, 3, 4, 5)]
     comp = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30)
     assert comp.perft_position(p, 1) == 17
     eng.close()
     comp.close()
 
 
-def test_readme_known_totals(gpu_engine):
+@pytest.mark.parametrize("leaf_kernel", [1, 2])
+def test_readme_known_totals(gpu_engine, leaf_kernel):
     # README.md:51-52 and :92 (RTX PRO 6000 / GB10 tables)
+    gpu_engine.set_tuning(leaf_kernel=leaf_kernel)
     assert gpu_engine.perft_position(pg.parse_fen(START), 8) == 84_998_978_956
     assert gpu_engine.perft_position(pg.parse_fen(KIWIPETE), 7) == 374_190_009_323
+    gpu_engine.set_tuning(leaf_kernel=2)
 
 
 def test_readme_startpos_perft9(gpu_engine):
