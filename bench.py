@@ -296,11 +296,15 @@ def main():
         sm_mhz = peaks.get("sm_max_mhz", 1965.0)
         issue_peak = 148 * 4 * sm_mhz * 1e6 / 1e9  # G warp-instructions / s
         inst_per_pos = consts.get("warp_inst_per_position")
+        dram_per_pos = consts.get("dram_bytes_per_position")
         roofline = {"bound": "int_issue", "unit": "Gwarp-inst/s", "peak": issue_peak,
-                    "peak_source": f"148 SMs x 4 issue/clk x sm_max_mhz ({peak_kind})",
+                    "peak_source": f"148 SMs x 4 warp-inst issue/clk x sm_max_mhz ({peak_kind})",
                     "kernel": "k_leaf2", "leaf_ms": my_leaf_ms, "positions_per_launch": leaf_pos,
                     "positions_per_s": leaf_pos / (my_leaf_ms / 1e3) if my_leaf_ms > 0 else None,
-                    "achieved": None, "frac": None, "traffic": consts.get("dram_bytes_per_launch")}
+                    "achieved": None, "frac": None,
+                    "traffic": dram_per_pos * leaf_pos if dram_per_pos else None,
+                    "traffic_note": "DRAM bytes per move-count call from the committed ncu capture "
+                                    "(profiles/), scaled by this launch's calls"}
         if inst_per_pos:
             ach = inst_per_pos * leaf_pos / (my_leaf_ms / 1e3) / 1e9
             roofline["achieved"] = ach

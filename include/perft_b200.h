@@ -91,6 +91,12 @@ int pb_device_count(void);
  * factor of pos and the arena size (estimateLaunchDepth, launcher.cu:533-562). */
 int pb_choose_launch_depth(pb_ctx *ctx, const pb_pos *pos);
 
+/* Replaces initTT (launcher.cu:128-351) for a run up to max_depth: fixes the
+ * launch depth (as pb_choose_launch_depth) and, in TT mode, sizes the host
+ * tables for remaining depths launch_depth..max_depth.  Device tables are
+ * sized on the first GPU call. */
+int pb_prepare(pb_ctx *ctx, const pb_pos *pos, int max_depth);
+
 /* Replaces perft_gpu_host_bfs (perft_kernels.cu:620-990): perft(depth) of one
  * position, the whole subtree on the GPU (the host only splits the root when
  * a level would not fit the arena). */

@@ -119,6 +119,7 @@ def _load() -> ctypes.CDLL:
         "pb_random_playout": (ctypes.c_int, [P(ctypes.c_uint64), ctypes.c_int, P(Pos)]),
         "pb_device_count": (ctypes.c_int, []),
         "pb_choose_launch_depth": (ctypes.c_int, [ctypes.c_void_p, P(Pos)]),
+        "pb_prepare": (ctypes.c_int, [ctypes.c_void_p, P(Pos), ctypes.c_int]),
         "pb_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
         "pb_set_tuning": (ctypes.c_int, [ctypes.c_void_p, P(Tuning)]),
         "pb_get_tuning": (ctypes.c_int, [ctypes.c_void_p, P(Tuning)]),
@@ -340,6 +341,9 @@ class Engine:
         st = Stats()
         self._check(lib.pb_last_stats(self._h, ctypes.byref(st)))
         return st
+
+    def prepare(self, p: Pos, max_depth: int) -> int:
+        return lib.pb_prepare(self._h, ctypes.byref(p), max_depth)
 
     def choose_launch_depth(self, p: Pos) -> int:
         return lib.pb_choose_launch_depth(self._h, ctypes.byref(p))

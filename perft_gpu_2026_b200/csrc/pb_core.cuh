@@ -348,16 +348,21 @@ PB_HD u32 count_moves(const Board &b, u32 state)
 
     u64 fp = my_pawns & ~pinned;
     u64 p1 = push1<C>(fp) & empty;
-    u64 promos = p1 & PROMO_RANKS;
-    n += popc(p1 ^ promos);
     n += popc(push1<C>(p1 & double_push_rank<C>()) & empty);
     u64 cw = cap_west<C>(fp) & s.them, ce = cap_east<C>(fp) & s.them;
-    u64 pw = cw & PROMO_RANKS, pe = ce & PROMO_RANKS;
-    n += popc(cw ^ pw) + popc(ce ^ pe);
-    if (STRICT)
-        n += 4 * (popc(promos) + popc(pw) + popc(pe));
-    else
-        n += 4 * popc(promos | pw | pe);
+    constexpr u64 RANK7 = C == WHITE ? 0x00FF000000000000ULL : 0x000000000000FF00ULL;
+    if (!(fp & RANK7)) {
+        // no pawn can promote: every push and capture is one move
+        n += popc(p1) + popc(cw) + popc(ce);
+    } else {
+        u64 promos = p1 & PROMO_RANKS;
+        u64 pw = cw & PROMO_RANKS, pe = ce & PROMO_RANKS;
+        n += popc(p1 ^ promos) + popc(cw ^ pw) + popc(ce ^ pe);
+        if (STRICT)
+            n += 4 * (popc(promos) + popc(pw) + popc(pe));
+        else
+            n += 4 * popc(promos | pw | pe);
+    }
 
     u32 castle = C == WHITE ? (state & 3) : ((state >> 2) & 3);
     if (castle) {

@@ -1,0 +1,294 @@
+// pb_devtt.cuh - device transposition tables and the TT-mode BFS kernels.
+//
+// One table per remaining depth r, like the reference's deviceTTs[r]
+// (tt.h:16-156, launcher.cu:128-351), but every hit is verified against the
+// full 128-bit key:
+//   r = 2, 3  ("shallow", 16 B): w1 = (lo << 24) | (count + 1), w0 = hi ^ w1.
+//             The slot is floor(lo * slots / 2^64), so a slot holds keys whose
+//             lo lies in an interval shorter than 2^40 when the table has at
+//             least 2^24 slots: lo's low 40 bits in w1 then pin lo exactly,
+//             and w0 ^ w1 gives the whole hi.
+//   r >= 4    ("deep", 32 B): {lo ^ c, hi ^ c, c, lo ^ hi ^ c}, one 256-bit
+//             store; a torn read cannot verify unless both halves carry the
+//             same key.
+// Replacement is always-overwrite (tt.h:60-70).
+//
+// TT-mode BFS (perft_kernels.cu:700-982): the expand kernel also derives each
+// child's key incrementally, probes TT[r] and marks hits (not expanded);
+// duplicates inside a level are expanded once (owner = smallest index among
+// equal 128-bit keys, elected with a 64-bit atomicMax); the leaf probes and
+// stores TT[2]; an upsweep then sums every position's children over its
+// contiguous child range, stores TT[r] and copies owners' counts to their
+// duplicates.
+#pragma once
+#include "pb_core.cuh"
+#include "pb_kernels.cuh"
+#include "pb_tt.cuh"
+
+namespace pb {
+
+enum { TT_NONE = 0, TT_SHALLOW = 1, TT_DEEP = 2 };
+constexpr int TT_MAX_DEPTH = 32;
+constexpr u64 SHALLOW_COUNT_MASK = 0xFFFFFFULL;
+
+struct TTView {
+    u64 *entries;  // SHALLOW: 2 words per slot, DEEP: 4 words per slot
+    u64 slots;     // any size: the slot is the high word of lo * slots
+    int kind;
+};
+
+__device__ __forceinline__ u64 tt_slot(const TTView &t, u64 lo) { return __umul64hi(lo, t.slots); }
+
+__device__ __forceinline__ bool tt_probe(const TTView &t, const Hash128 &h, u64 *out)
+{
+    if (t.kind == TT_NONE) return false;
+    u64 slot = tt_slot(t, h.lo);
+    if (t.kind == TT_SHALLOW) {
+        u64 w0, w1;
+        asm volatile("ld.global.v2.u64 {%0,%1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(t.entries + 2 * slot));
+        if ((w0 ^ w1) == h.hi && ((w1 ^ (h.lo << 24)) & ~SHALLOW_COUNT_MASK) == 0 && (w1 & SHALLOW_COUNT_MASK)) {
+            *out = (w1 & SHALLOW_COUNT_MASK) - 1;
+            return true;
+        }
+        return false;
+    }
+    u64 w0, w1, w2, w3;
+    asm volatile("ld.global.v4.u64 {%0,%1,%2,%3}, [%4];"
+                 : "=l"(w0), "=l"(w1), "=l"(w2), "=l"(w3)
+                 : "l"(t.entries + 4 * slot));
+    if ((w0 ^ w2) == h.lo && (w1 ^ w2) == h.hi && (w3 ^ w2) == (h.lo ^ h.hi) && (w0 | w1 | w2 | w3)) {
+        *out = w2;
+        return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tt_store(const TTView &t, const Hash128 &h, u64 count)
+{
+    if (t.kind == TT_NONE) return;
+    u64 slot = tt_slot(t, h.lo);
+    if (t.kind == TT_SHALLOW) {
+        if (count + 1 > SHALLOW_COUNT_MASK) return;  // never truncate a count
+        u64 w1 = (h.lo << 24) | (count + 1);
+        u64 w0 = h.hi ^ w1;
+        asm volatile("st.global.v2.u64 [%0], {%1,%2};" ::"l"(t.entries + 2 * slot), "l"(w0), "l"(w1) : "memory");
+        return;
+    }
+    asm volatile("st.global.v4.u64 [%0], {%1,%2,%3,%4};" ::"l"(t.entries + 4 * slot), "l"(h.lo ^ count),
+                 "l"(h.hi ^ count), "l"(count), "l"(h.lo ^ h.hi ^ count)
+                 : "memory");
+}
+
+struct TTViews {
+    TTView v[TT_MAX_DEPTH];
+};
+
+// Device tables, one per remaining depth in [2, max_depth].
+struct DeviceTT {
+    TTViews views{};
+    std::vector<void *> blocks;
+    u64 bytes = 0;
+
+    bool ready() const { return !blocks.empty(); }
+
+    // budget_mb 0 = auto (a share of `free_bytes`).  Depth 2 and 3 get the
+    // shallow format; the split gives the leaf table (depth 2) a quarter,
+    // depth 3 a quarter and the rest to depths 4..max_depth-1.
+    int init(int budget_mb, size_t free_bytes, int max_depth, int verbose, std::string *err)
+    {
+        release();
+        u64 budget = budget_mb > 0 ? (u64)budget_mb << 20 : (u64)(free_bytes * 0.85);
+        if (max_depth < 3) max_depth = 3;
+        if (max_depth > TT_MAX_DEPTH - 1) max_depth = TT_MAX_DEPTH - 1;
+        int deep = max_depth - 4 + 1;  // depths 4..max_depth
+        for (int r = 2; r <= max_depth; r++) {
+            double share = (r <= 3) ? 0.25 : (deep > 0 ? 0.5 / deep : 0.0);
+            if (deep <= 0 && r <= 3) share = 0.5;
+            u64 want = (u64)(budget * share);
+            bool shallow = r <= 3;
+            u64 esz = shallow ? 16 : 32;
+            u64 slots = want / esz;
+            if (shallow && slots < (1ULL << 24)) continue;  // too small for key verification
+            if (!shallow && slots < 1024) continue;
+            void *p = nullptr;
+            if (cudaMalloc(&p, slots * esz) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            cudaMemset(p, 0, slots * esz);
+            blocks.push_back(p);
+            views.v[r] = TTView{reinterpret_cast<u64 *>(p), slots, shallow ? TT_SHALLOW : TT_DEEP};
+            bytes += slots * esz;
+            if (verbose)
+                printf("Device TT[%d]%s: %lluM entries (%llu MB)\n", r, shallow ? " (shallow)" : "",
+                       (unsigned long long)(slots >> 20), (unsigned long long)((slots * esz) >> 20));
+        }
+        (void)err;
+        return 0;
+    }
+    void clear()
+    {
+        for (int r = 0; r < TT_MAX_DEPTH; r++)
+            if (views.v[r].kind != TT_NONE)
+                cudaMemset(views.v[r].entries, 0, views.v[r].slots * (views.v[r].kind == TT_SHALLOW ? 16 : 32));
+    }
+    void release()
+    {
+        for (void *p : blocks) cudaFree(p);
+        blocks.clear();
+        views = TTViews{};
+        bytes = 0;
+    }
+    TTView at(int r) const { return (r >= 0 && r < TT_MAX_DEPTH) ? views.v[r] : TTView{nullptr, 0, TT_NONE}; }
+};
+
+// ---------------------------------------------------------------- TT-mode kernels
+enum : uint8_t { PF_HIT = 1, PF_DUP = 2 };
+
+// Expand with keys: child board/state/key, TT[r] probe, exact child count
+// (0 on a hit, the hit value in vals[i]).
+template <int C>
+__global__ void __launch_bounds__(256) k_expand_count_tt(const Board *__restrict__ pboards,
+                                                         const uint8_t *__restrict__ pstates,
+                                                         const Hash128 *__restrict__ phash,
+                                                         const u32 *__restrict__ pidx,
+                                                         const uint16_t *__restrict__ moves, u64 n, u64 nparents,
+                                                         TTView tt, Board *__restrict__ cboards,
+                                                         uint8_t *__restrict__ cstates, Hash128 *__restrict__ chash,
+                                                         u32 *__restrict__ counts, u64 *__restrict__ vals,
+                                                         uint8_t *__restrict__ flags, u32 *__restrict__ err)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    u32 p = pidx[i];
+    if (p >= nparents) {
+        atomicOr(err, DEVERR_CAPACITY);
+        counts[i] = 0;
+        flags[i] = PF_HIT;
+        vals[i] = 0;
+        return;
+    }
+    Board b = load_board(pboards + p);
+    u32 st = pstates[p];
+    Board before = b;
+    uint16_t mv = moves[i];
+    make_move<C>(b, st, mv);
+    Hash128 h = hash_move(phash[p], before, pstates[p], st, C, mv);
+    store_board(cboards + i, b);
+    cstates[i] = (uint8_t)st;
+    chash[i] = h;
+    u64 hit;
+    if (tt_probe(tt, h, &hit)) {
+        counts[i] = 0;
+        vals[i] = hit;
+        flags[i] = PF_HIT;
+    } else {
+        counts[i] = count_moves<1 - C, true>(b, st);
+        vals[i] = 0;
+        flags[i] = 0;
+    }
+}
+
+// Duplicate election inside a level: slot word = (generation << 32) | ~index;
+// atomicMax keeps the current generation and the smallest index.
+__global__ void k_dedup_claim(const Hash128 *__restrict__ h, const uint8_t *__restrict__ flags, u64 n,
+                              unsigned long long *__restrict__ slots, u64 mask, u32 gen)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (flags[i] & PF_HIT)) return;
+    unsigned long long w = ((unsigned long long)gen << 32) | (unsigned long long)(~(u32)i);
+    atomicMax(slots + (h[i].lo & mask), w);
+}
+
+__global__ void k_dedup_resolve(const Hash128 *__restrict__ h, uint8_t *__restrict__ flags, u64 n,
+                                const unsigned long long *__restrict__ slots, u64 mask, u32 gen,
+                                u32 *__restrict__ counts, u32 *__restrict__ redirect)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (flags[i] & PF_HIT)) return;
+    unsigned long long w = slots[h[i].lo & mask];
+    if ((u32)(w >> 32) != gen) return;
+    u32 owner = ~(u32)w;
+    if (owner == (u32)i || owner >= n) return;
+    Hash128 a = h[i], o = h[owner];
+    if (a.lo == o.lo && a.hi == o.hi) {
+        flags[i] |= PF_DUP;
+        counts[i] = 0;
+        redirect[i] = owner;
+    }
+}
+
+// Leaf with the depth-2 table: perft 2 of each edge's child, per edge.
+template <int C, bool STRICT>
+__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
+    k_leaf2_tt(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+               const Hash128 *__restrict__ phash, const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
+               u64 n, u64 nparents, TTView tt, u32 *__restrict__ out, unsigned long long *__restrict__ counter)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    u32 total = 0, counted = 0;
+    if (i < n && pidx[i] < nparents) {
+        u32 p = pidx[i];
+        Board b = load_board(pboards + p);
+        u32 st = pstates[p];
+        Board before = b;
+        uint16_t mv0 = moves[i];
+        make_move<C>(b, st, mv0);
+        Hash128 h = hash_move(phash[p], before, pstates[p], st, C, mv0);
+        u64 hit;
+        if (tt_probe(tt, h, &hit)) {
+            total = (u32)hit;
+        } else {
+            uint16_t mv[MAX_MOVES];
+            ArraySink sink{mv, 0};
+            gen_moves<1 - C>(b, st, sink);
+            for (int k = 0; k < sink.n; k++) {
+                Board g = b;
+                u32 gs = st;
+                make_move<1 - C>(g, gs, mv[k]);
+                total += count_moves<C, STRICT>(g, gs);
+            }
+            counted = sink.n;
+            tt_store(tt, h, total);
+        }
+        out[i] = total;
+    }
+    counted = __reduce_add_sync(0xffffffffu, counted);
+    if ((threadIdx.x & 31) == 0 && counted) atomicAdd(counter + 1, (unsigned long long)counted);
+}
+
+// Upsweep of one level: vals[i] = sum of the children's counts over
+// [offs[i], offs[i] + counts[i]) unless i was a TT hit or a duplicate; the
+// result is stored in TT[r].
+template <class ChildT>
+__global__ void k_upsweep(const ChildT *__restrict__ child, const u64 *__restrict__ offs,
+                          const u32 *__restrict__ counts, const uint8_t *__restrict__ flags,
+                          const Hash128 *__restrict__ h, u64 n, TTView tt, u64 *__restrict__ vals)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || flags[i]) return;
+    u64 a = offs[i], z = a + counts[i], s = 0;
+    for (u64 k = a; k < z; k++) s += (u64)child[k];
+    vals[i] = s;
+    tt_store(tt, h[i], s);
+}
+
+__global__ void k_resolve_dups(const uint8_t *__restrict__ flags, const u32 *__restrict__ redirect, u64 n,
+                               u64 *__restrict__ vals)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !(flags[i] & PF_DUP)) return;
+    vals[i] = vals[redirect[i]];
+}
+
+template <class T>
+__global__ void k_sum(const T *__restrict__ v, u64 n, unsigned long long *__restrict__ out)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long x = (i < n) ? (unsigned long long)v[i] : 0ULL;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(out, x);
+}
+
+}  // namespace pb

@@ -25,6 +25,7 @@
 #include "pb_util.cuh"
 #include "pb_kernels.cuh"
 #include "pb_tt.cuh"
+#include "pb_devtt.cuh"
 
 using namespace pb;
 
@@ -53,6 +54,10 @@ struct pb_ctx {
     pb_stats stats{};
     HostTT htt;
     DeviceTT dtt;
+    int dtt_max_depth = 0;
+    size_t dtt_free_bytes = 0;
+    u32 dedup_gen = 0;
+    int htt_last = 0;
     std::string err;
 };
 
@@ -147,11 +152,11 @@ inline unsigned grid_for(u64 n, int threads) { return (unsigned)((n + threads - 
 enum { BFS_OK = 0, BFS_TOO_BIG = 1 };
 
 template <int C, bool S>
-int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi, const uint16_t *mv, u64 n)
+int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi, const uint16_t *mv, u64 n, u64 npar)
 {
     cudaStream_t s = ctx->stream;
     if (ctx->tuning.leaf_kernel == 1) {
-        k_leaf2<C, S><<<grid_for(n, PB_LEAF_THREADS), PB_LEAF_THREADS, 0, s>>>(b, st, pi, mv, n, ctx->d_counter);
+        k_leaf2<C, S><<<grid_for(n, PB_LEAF_THREADS), PB_LEAF_THREADS, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter);
         PB_CUDA(cudaGetLastError());
         return PB_OK;
     }
@@ -163,17 +168,18 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
     }
     u64 grid = std::min<u64>(nchunks, (u64)ctx->num_sms * per_sm);
     if (grid > ctx->spill_blocks) return fail(ctx, PB_ERR_NOMEM, "leaf spill area too small");
-    k_leaf2_coop<C, S><<<(unsigned)grid, LEAF_T, 0, s>>>(b, st, pi, mv, n, ctx->spill, ctx->d_counter);
+    k_leaf2_coop<C, S><<<(unsigned)grid, LEAF_T, 0, s>>>(b, st, pi, mv, n, npar, ctx->spill, ctx->d_counter);
     PB_CUDA(cudaGetLastError());
     return PB_OK;
 }
 
 int launch_leaf(pb_ctx *ctx, int c, bool strict, const Board *b, const uint8_t *st, const u32 *pi,
-                const uint16_t *mv, u64 n)
+                const uint16_t *mv, u64 n, u64 npar)
 {
-    if (c == WHITE) return strict ? launch_leaf_t<WHITE, true>(ctx, b, st, pi, mv, n)
-                                  : launch_leaf_t<WHITE, false>(ctx, b, st, pi, mv, n);
-    return strict ? launch_leaf_t<BLACK, true>(ctx, b, st, pi, mv, n) : launch_leaf_t<BLACK, false>(ctx, b, st, pi, mv, n);
+    if (c == WHITE) return strict ? launch_leaf_t<WHITE, true>(ctx, b, st, pi, mv, n, npar)
+                                  : launch_leaf_t<WHITE, false>(ctx, b, st, pi, mv, n, npar);
+    return strict ? launch_leaf_t<BLACK, true>(ctx, b, st, pi, mv, n, npar)
+                  : launch_leaf_t<BLACK, false>(ctx, b, st, pi, mv, n, npar);
 }
 
 // One GPU breadth-first perft; status BFS_TOO_BIG when a level would not fit.
@@ -215,6 +221,7 @@ int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth,
     Board *cur_b = pb_;
     uint8_t *cur_s = ps;
     u64 n = (u64)n0;
+    u64 n_par = 1;  // positions the current edges point into
     int c = color;
     for (int rem = depth - 1; rem > 2; rem--) {
         Board *cb = ar.take<Board>(n);
@@ -228,9 +235,9 @@ int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth,
             return PB_OK;
         }
         if (c == WHITE)
-            k_expand_count<WHITE><<<grid_for(n, 256), 256, 0, s>>>(cur_b, cur_s, epi, emv, n, cb, cs, cnt);
+            k_expand_count<WHITE><<<grid_for(n, 256), 256, 0, s>>>(cur_b, cur_s, epi, emv, n, n_par, cb, cs, cnt, ctx->d_err);
         else
-            k_expand_count<BLACK><<<grid_for(n, 256), 256, 0, s>>>(cur_b, cur_s, epi, emv, n, cb, cs, cnt);
+            k_expand_count<BLACK><<<grid_for(n, 256), 256, 0, s>>>(cur_b, cur_s, epi, emv, n, n_par, cb, cs, cnt, ctx->d_err);
         PB_CUDA(cudaGetLastError());
         PB_CUDA(cudaMemsetAsync(status, 0, sizeof(u64) * tiles, s));
         PB_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s));
@@ -260,21 +267,22 @@ int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth,
             return PB_OK;
         }
         if (c == WHITE)
-            k_generate<BLACK><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n, nmv, npi);
+            k_generate<BLACK><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n, nmv, npi, ctx->d_err);
         else
-            k_generate<WHITE><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n, nmv, npi);
+            k_generate<WHITE><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n, nmv, npi, ctx->d_err);
         PB_CUDA(cudaGetLastError());
         stats.kernels += 1;
         cur_b = cb;
         cur_s = cs;
         emv = nmv;
         epi = npi;
+        n_par = n;
         n = next;
         c = 1 - c;
     }
     PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(unsigned long long), s));
     if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[1], s));
-    int rc = launch_leaf(ctx, c, strict, cur_b, cur_s, epi, emv, n);
+    int rc = launch_leaf(ctx, c, strict, cur_b, cur_s, epi, emv, n, n_par);
     if (rc != PB_OK) return rc;
     PB_CUDA(cudaGetLastError());
     if (ctx->timing) {
@@ -300,13 +308,235 @@ int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth,
     return PB_OK;
 }
 
+// Device tables for remaining depths 2..max_r (allocated on first use, kept
+// for the context's lifetime like the reference's initTT).
+int ensure_dtt(pb_ctx *ctx, int max_r)
+{
+    if (max_r < 3) max_r = 3;
+    if (ctx->dtt.ready() && ctx->dtt_max_depth >= max_r) return PB_OK;
+    // (re)size for depths 2..max_r; a deeper call than prepared drops the
+    // current contents, which only costs hits
+    ctx->dtt.init(ctx->opts.device_tt_mb, ctx->dtt_free_bytes, max_r, ctx->opts.verbose, &ctx->err);
+    ctx->dtt_max_depth = max_r;
+    return PB_OK;
+}
+
+struct TTLevel {
+    Hash128 *hash;
+    u32 *counts;
+    u64 *vals;
+    uint8_t *flags;
+    u32 *redirect;
+    u64 *offs;
+    u64 n;
+    int rem;
+};
+
+// One GPU breadth-first perft with the device TTs (perft_gpu_host_bfs with
+// g_useTT, perft_kernels.cu:620-990): probe at every level, dedup, leaf TT,
+// then the upsweep stores every level's counts.
+int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth, const Hash128 &root_hash,
+                 u64 *out, int *bfs_status)
+{
+    *bfs_status = BFS_OK;
+    const bool strict = ctx->opts.strict != 0;
+    if (depth <= 2) {
+        *out = host_perft(root, root_st, color, depth, strict);
+        return PB_OK;
+    }
+    int rc = ensure_dtt(ctx, depth - 1);
+    if (rc != PB_OK) return rc;
+    uint16_t root_moves[MAX_MOVES];
+    int n0 = host_gen(root, root_st, color, root_moves);
+    if (n0 == 0) {
+        *out = 0;
+        return PB_OK;
+    }
+    cudaStream_t s = ctx->stream;
+    pb_stats &stats = ctx->stats;
+    Arena ar{ctx->arena, ctx->arena_bytes};
+    Board *pb_ = ar.take<Board>(1);
+    uint8_t *ps = ar.take<uint8_t>(1);
+    Hash128 *ph = ar.take<Hash128>(1);
+    uint16_t *emv = ar.take<uint16_t>(n0);
+    u32 *epi = ar.take<u32>(n0);
+    if (!pb_ || !ps || !ph || !emv || !epi) {
+        *bfs_status = BFS_TOO_BIG;
+        return PB_OK;
+    }
+    uint8_t st8 = (uint8_t)root_st;
+    PB_CUDA(cudaMemcpyAsync(pb_, &root, sizeof(Board), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(ps, &st8, 1, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(ph, &root_hash, sizeof(Hash128), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(emv, root_moves, sizeof(uint16_t) * n0, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemsetAsync(epi, 0, sizeof(u32) * n0, s));
+    PB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s));
+    stats.h2d_bytes += sizeof(Board) + 1 + sizeof(Hash128) + sizeof(uint16_t) * n0;
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[0], s));
+
+    std::vector<TTLevel> levels;
+    Board *cur_b = pb_;
+    uint8_t *cur_s = ps;
+    Hash128 *cur_h = ph;
+    u64 n = (u64)n0, n_par = 1;
+    int c = color;
+    for (int rem = depth - 1; rem > 2; rem--) {
+        TTLevel L{};
+        Board *cb = ar.take<Board>(n);
+        uint8_t *cs = ar.take<uint8_t>(n);
+        L.hash = ar.take<Hash128>(n);
+        L.counts = ar.take<u32>(n);
+        L.vals = ar.take<u64>(n);
+        L.flags = ar.take<uint8_t>(n);
+        L.redirect = ar.take<u32>(n);
+        L.offs = ar.take<u64>(n);
+        u64 dsz = 1;
+        while (dsz < 2 * n) dsz *= 2;
+        unsigned long long *slots = ar.take<unsigned long long>(dsz);
+        u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+        u64 *status = ar.take<u64>(tiles);
+        if (!cb || !cs || !L.hash || !L.counts || !L.vals || !L.flags || !L.redirect || !L.offs || !slots || !status) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        L.n = n;
+        L.rem = rem;
+        TTView tv = ctx->dtt.at(rem);
+        unsigned g = grid_for(n, 256);
+        if (c == WHITE)
+            k_expand_count_tt<WHITE><<<g, 256, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, cb, cs, L.hash,
+                                                       L.counts, L.vals, L.flags, ctx->d_err);
+        else
+            k_expand_count_tt<BLACK><<<g, 256, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, cb, cs, L.hash,
+                                                       L.counts, L.vals, L.flags, ctx->d_err);
+        PB_CUDA(cudaGetLastError());
+        PB_CUDA(cudaMemsetAsync(slots, 0, sizeof(unsigned long long) * dsz, s));
+        u32 gen = ++ctx->dedup_gen;
+        k_dedup_claim<<<g, 256, 0, s>>>(L.hash, L.flags, n, slots, dsz - 1, gen);
+        k_dedup_resolve<<<g, 256, 0, s>>>(L.hash, L.flags, n, slots, dsz - 1, gen, L.counts, L.redirect);
+        PB_CUDA(cudaGetLastError());
+        PB_CUDA(cudaMemsetAsync(status, 0, sizeof(u64) * tiles, s));
+        PB_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s));
+        k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(L.counts, n, L.offs, status, ctx->d_ticket, ctx->d_total,
+                                                         ctx->d_err);
+        PB_CUDA(cudaGetLastError());
+        PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_total, sizeof(u64), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 1, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+        stats.kernels += 4;
+        stats.d2h_bytes += 12;
+        if ((u32)ctx->h_pinned[1]) return fail(ctx, PB_ERR_DEVICE, "TT level reported a device error");
+        u64 next = ctx->h_pinned[0];
+        stats.levels++;
+        if (stats.levels < 16) stats.level_sizes[stats.levels] = next;
+        levels.push_back(L);
+        cur_b = cb;
+        cur_s = cs;
+        cur_h = L.hash;
+        n_par = n;
+        c = 1 - c;
+        if (next == 0) {
+            n = 0;
+            break;
+        }
+        if (next > 0xFFFFFFFFULL) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        uint16_t *nmv = ar.take<uint16_t>(next);
+        u32 *npi = ar.take<u32>(next);
+        if (!nmv || !npi) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        if (c == WHITE)
+            k_generate<WHITE><<<grid_for(n_par, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, L.offs, ctx->d_total, n_par,
+                                                                                   nmv, npi, ctx->d_err);
+        else
+            k_generate<BLACK><<<grid_for(n_par, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, L.offs, ctx->d_total, n_par,
+                                                                                   nmv, npi, ctx->d_err);
+        PB_CUDA(cudaGetLastError());
+        stats.kernels += 1;
+        emv = nmv;
+        epi = npi;
+        n = next;
+    }
+    // leaf: per-edge perft(2) with the depth-2 table
+    u32 *leafcnt = ar.take<u32>(n > 0 ? n : 1);
+    if (!leafcnt) {
+        *bfs_status = BFS_TOO_BIG;
+        return PB_OK;
+    }
+    PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(unsigned long long), s));
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[1], s));
+    if (n > 0) {
+        TTView tv = ctx->dtt.at(2);
+        unsigned g = grid_for(n, PB_LEAF_THREADS);
+        if (c == WHITE) {
+            if (strict)
+                k_leaf2_tt<WHITE, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, leafcnt, ctx->d_counter);
+            else
+                k_leaf2_tt<WHITE, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, leafcnt, ctx->d_counter);
+        } else {
+            if (strict)
+                k_leaf2_tt<BLACK, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, leafcnt, ctx->d_counter);
+            else
+                k_leaf2_tt<BLACK, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, leafcnt, ctx->d_counter);
+        }
+        PB_CUDA(cudaGetLastError());
+        stats.kernels += 1;
+    }
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[2], s));
+    // upsweep
+    const u32 *child32 = leafcnt;
+    const u64 *child64 = nullptr;
+    for (int li = (int)levels.size() - 1; li >= 0; li--) {
+        TTLevel &L = levels[li];
+        unsigned g = grid_for(L.n, 256);
+        TTView tv = ctx->dtt.at(L.rem);
+        if (child64)
+            k_upsweep<u64><<<g, 256, 0, s>>>(child64, L.offs, L.counts, L.flags, L.hash, L.n, tv, L.vals);
+        else
+            k_upsweep<u32><<<g, 256, 0, s>>>(child32, L.offs, L.counts, L.flags, L.hash, L.n, tv, L.vals);
+        k_resolve_dups<<<g, 256, 0, s>>>(L.flags, L.redirect, L.n, L.vals);
+        PB_CUDA(cudaGetLastError());
+        stats.kernels += 2;
+        child64 = L.vals;
+    }
+    PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
+    if (levels.empty())
+        k_sum<u32><<<grid_for(n, 256), 256, 0, s>>>(leafcnt, n, ctx->d_counter);
+    else
+        k_sum<u64><<<grid_for(levels[0].n, 256), 256, 0, s>>>(levels[0].vals, levels[0].n, ctx->d_counter);
+    PB_CUDA(cudaGetLastError());
+    stats.kernels += 1;
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[3], s));
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_counter, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 2, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    if ((u32)ctx->h_pinned[2]) return fail(ctx, PB_ERR_DEVICE, "TT kernel reported a device error");
+    *out = ctx->h_pinned[0];
+    stats.leaf_edges += n;
+    stats.leaf_positions += ctx->h_pinned[1];
+    stats.d2h_bytes += 20;
+    if (ctx->timing) {
+        float a = 0, b2 = 0;
+        PB_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[3]));
+        PB_CUDA(cudaEventElapsedTime(&b2, ctx->ev[1], ctx->ev[2]));
+        stats.device_ms += a;
+        stats.leaf_ms += b2;
+    }
+    return PB_OK;
+}
+
 // perft of one position on the GPU; a level too big for the arena splits the
 // root on the host and recurses (the reference's OOM path recomputes one
 // level down the same way, launcher.cu:600-610, but on the CPU).
 int gpu_perft(pb_ctx *ctx, const Board &b, u32 st, int c, int depth, u64 *out)
 {
     int status = BFS_OK;
-    int rc = bfs_perft(ctx, b, st, c, depth, out, &status);
+    int rc = ctx->opts.use_tt ? bfs_perft_tt(ctx, b, st, c, depth, hash_position(b, st, c), out, &status)
+                              : bfs_perft(ctx, b, st, c, depth, out, &status);
     if (rc != PB_OK) return rc;
     if (status == BFS_OK) return PB_OK;
     if (depth <= 3) return fail(ctx, PB_ERR_NOMEM, "BFS arena too small for a depth-3 perft");
@@ -452,10 +682,9 @@ int pb_create(int device, const pb_opts *opts, pb_ctx **out)
             }
             if ((e = cudaMalloc(&ctx->arena, want)) != cudaSuccess) { rc = cuda_fail(ctx, e, "arena"); break; }
             ctx->arena_bytes = want;
-            if (ctx->opts.use_tt) {
-                rc = ctx->dtt.init(ctx->opts.device_tt_mb, freeb > want ? freeb - want : 0, ctx->opts.verbose, &ctx->err);
-                if (rc != PB_OK) break;
-            }
+            build_zobrist();
+            if ((e = cudaMemcpyToSymbol(g_zob, &h_zob, sizeof(Zobrist))) != cudaSuccess) { rc = cuda_fail(ctx, e, "upload keys"); break; }
+            ctx->dtt_free_bytes = freeb > want + (4ULL << 30) ? freeb - want - (4ULL << 30) : 0;
         } while (0);
         if (rc != PB_OK) {
             std::string msg = ctx->err;
@@ -603,13 +832,36 @@ int pb_choose_launch_depth(pb_ctx *ctx, const pb_pos *pos)
     return ctx->launch_depth;
 }
 
+int pb_prepare(pb_ctx *ctx, const pb_pos *pos, int max_depth)
+{
+    if (!ctx || !pos || max_depth < 0 || max_depth > 30) return PB_ERR_ARG;
+    // With tables the BFS levels shrink (hits and duplicates are not
+    // expanded), so deep runs call the GPU one ply higher, as the reference
+    // does for perft 10 and beyond (perft.cu:126-130).
+    if (ctx->gpu && ctx->opts.use_tt && ctx->opts.launch_depth <= 0 && !ctx->launch_depth && max_depth >= 10)
+        ctx->launch_depth = std::max(estimate_launch_depth(ctx, to_board(*pos), pos->state, pos->color), 9);
+    int ld = pb_choose_launch_depth(ctx, pos);
+    if (ctx->gpu && ctx->opts.use_tt) {
+        int rc = ensure_dtt(ctx, std::min(ld, max_depth) - 1);
+        if (rc != PB_OK) return rc;
+    }
+    if (ctx->opts.use_tt && (!ctx->htt.ready() || ctx->htt_last < max_depth)) {
+        ctx->htt.init(ctx->opts.host_tt_mb, ld, max_depth);
+        ctx->htt_last = max_depth;
+    }
+    return ld;
+}
+
 int pb_perft_launch(pb_ctx *ctx, const pb_pos *pos, int depth, pb_u128 *count, double *seconds)
 {
     if (!ctx || !pos || !count || depth < 0 || depth > 30) return PB_ERR_ARG;
     if (ctx->gpu) PB_CUDA(cudaSetDevice(ctx->device));
     Board b = to_board(*pos);
     pb_choose_launch_depth(ctx, pos);
-    if (ctx->opts.use_tt && !ctx->htt.ready()) ctx->htt.init(ctx->opts.host_tt_mb, ctx->launch_depth, depth);
+    if (ctx->opts.use_tt && (!ctx->htt.ready() || ctx->htt_last < depth)) {
+        ctx->htt.init(ctx->opts.host_tt_mb, ctx->launch_depth, depth);
+        ctx->htt_last = depth;
+    }
     auto t0 = std::chrono::steady_clock::now();
     pb_u128 r{0, 0};
     int rc;
@@ -631,6 +883,7 @@ int pb_perft(pb_ctx *ctx, const char *fen, int max_depth, pb_u128 *per_depth, do
     if (!ctx || !fen || !per_depth || max_depth < 1 || max_depth > 30) return PB_ERR_ARG;
     pb_pos pos;
     if (!parse_fen(fen, &pos)) return fail(ctx, PB_ERR_FEN, "invalid FEN");
+    pb_prepare(ctx, &pos, max_depth);
     for (int d = 1; d <= max_depth; d++) {
         double secs = 0;
         int rc = pb_perft_launch(ctx, &pos, d, &per_depth[d - 1], &secs);

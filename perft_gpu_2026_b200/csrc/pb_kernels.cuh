@@ -50,13 +50,18 @@ template <int C>
 __global__ void __launch_bounds__(256) k_expand_count(const Board *__restrict__ pboards,
                                                       const uint8_t *__restrict__ pstates,
                                                       const u32 *__restrict__ pidx,
-                                                      const uint16_t *__restrict__ moves, u64 n,
+                                                      const uint16_t *__restrict__ moves, u64 n, u64 nparents,
                                                       Board *__restrict__ cboards, uint8_t *__restrict__ cstates,
-                                                      u32 *__restrict__ counts)
+                                                      u32 *__restrict__ counts, u32 *__restrict__ err)
 {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     u32 p = pidx[i];
+    if (p >= nparents) {  // only after a count/generation mismatch upstream
+        atomicOr(err, DEVERR_CAPACITY);
+        counts[i] = 0;
+        return;
+    }
     Board b = load_board(pboards + p);
     u32 st = pstates[p];
     make_move<C>(b, st, moves[i]);
@@ -169,15 +174,24 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(const u32 *__restrict__ i
 constexpr int GEN_THREADS = 128;
 constexpr int GEN_CAP = 8192;  // moves staged per CTA (6 B each = 48 KB)
 
+// Both sinks stop at `cap` moves: the level was sized with the exact count,
+// so more moves than that means the count and the generator disagree; the
+// excess is dropped and reported through the error word instead of being
+// written past the allocation.
 struct SmemSink {
     uint16_t *mv;
     u32 *pi;
     u32 parent;
-    int n;
+    int n, cap;
+    bool over;
     __device__ __forceinline__ void put(uint16_t m)
     {
-        mv[n] = m;
-        pi[n] = parent;
+        if (n < cap) {
+            mv[n] = m;
+            pi[n] = parent;
+        } else {
+            over = true;
+        }
         n++;
     }
 };
@@ -185,11 +199,16 @@ struct GlobalSink {
     uint16_t *mv;
     u32 *pi;
     u32 parent;
-    u64 n;
+    u64 n, cap;
+    bool over;
     __device__ __forceinline__ void put(uint16_t m)
     {
-        mv[n] = m;
-        pi[n] = parent;
+        if (n < cap) {
+            mv[n] = m;
+            pi[n] = parent;
+        } else {
+            over = true;
+        }
         n++;
     }
 };
@@ -199,7 +218,7 @@ __global__ void __launch_bounds__(GEN_THREADS) k_generate(const Board *__restric
                                                           const uint8_t *__restrict__ states,
                                                           const u64 *__restrict__ offs, const u64 *__restrict__ total,
                                                           u64 n, uint16_t *__restrict__ out_mv,
-                                                          u32 *__restrict__ out_pi)
+                                                          u32 *__restrict__ out_pi, u32 *__restrict__ err)
 {
     __shared__ uint16_t s_mv[GEN_CAP];
     __shared__ u32 s_pi[GEN_CAP];
@@ -212,13 +231,21 @@ __global__ void __launch_bounds__(GEN_THREADS) k_generate(const Board *__restric
     if (i < n) {
         Board b = load_board(boards + i);
         u32 st = states[i];
-        if (staged) {
-            SmemSink s{s_mv, s_pi, (u32)i, (int)(offs[i] - tile_begin)};
+        const u64 mine_begin = offs[i];
+        const u64 mine_end = (i + 1 < n) ? offs[i + 1] : *total;
+        bool over = false;
+        if (mine_end == mine_begin) {
+            // no moves allotted: mate, stalemate, a TT hit or a duplicate
+        } else if (staged) {
+            SmemSink s{s_mv, s_pi, (u32)i, (int)(mine_begin - tile_begin), (int)(mine_end - tile_begin), false};
             gen_moves<C>(b, st, s);
+            over = s.over || s.n != s.cap;
         } else {
-            GlobalSink s{out_mv, out_pi, (u32)i, offs[i]};
+            GlobalSink s{out_mv, out_pi, (u32)i, mine_begin, mine_end, false};
             gen_moves<C>(b, st, s);
+            over = s.over || s.n != s.cap;
         }
+        if (over) atomicOr(err, DEVERR_CAPACITY);
     }
     if (!staged) return;
     __syncthreads();
@@ -234,11 +261,11 @@ __global__ void __launch_bounds__(GEN_THREADS) k_generate(const Board *__restric
 template <int C>
 __global__ void __launch_bounds__(256) k_leaf1(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                                                const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves, u64 n,
-                                               unsigned long long *__restrict__ counter)
+                                               u64 nparents, unsigned long long *__restrict__ counter)
 {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     u32 cnt = 0;
-    if (i < n) {
+    if (i < n && pidx[i] < nparents) {
         u32 p = pidx[i];
         Board b = load_board(pboards + p);
         u32 st = pstates[p];
@@ -263,11 +290,11 @@ __global__ void __launch_bounds__(256) k_leaf1(const Board *__restrict__ pboards
 template <int C, bool STRICT>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS) k_leaf2(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                                                const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves, u64 n,
-                                               unsigned long long *__restrict__ counter)
+                                               u64 nparents, unsigned long long *__restrict__ counter)
 {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     u32 total = 0, counted = 0;
-    if (i < n) {
+    if (i < n && pidx[i] < nparents) {
         u32 p = pidx[i];
         Board b = load_board(pboards + p);
         u32 st = pstates[p];
@@ -332,7 +359,7 @@ template <int C, bool STRICT>
 __global__ void __launch_bounds__(LEAF_T, 4) k_leaf2_coop(const Board *__restrict__ pboards,
                                                           const uint8_t *__restrict__ pstates,
                                                           const u32 *__restrict__ pidx,
-                                                          const uint16_t *__restrict__ moves, u64 n,
+                                                          const uint16_t *__restrict__ moves, u64 n, u64 nparents,
                                                           uint16_t *__restrict__ spill,
                                                           unsigned long long *__restrict__ counter)
 {
@@ -351,7 +378,7 @@ __global__ void __launch_bounds__(LEAF_T, 4) k_leaf2_coop(const Board *__restric
         // ---- phase A: child position and its move list
         const u64 e = chunk * LEAF_T + tid;
         int cnt = 0;
-        if (e < n) {
+        if (e < n && pidx[e] < nparents) {
             u32 p = pidx[e];
             Board b = load_board(pboards + p);
             u32 st = pstates[p];

@@ -198,10 +198,5 @@ struct HostTT {
     }
 };
 
-// Device TT descriptor (filled in by pb_devtt.cuh when TT mode runs on GPU).
-struct DeviceTT {
-    int init(int, size_t, int, std::string *) { return 0; }
-    void release() {}
-};
 
 }  // namespace pb

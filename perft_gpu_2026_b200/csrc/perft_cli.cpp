@@ -118,7 +118,7 @@ int main(int argc, char **argv)
         fprintf(stderr, "init failed (%d)\n", rc);
         return 1;
     }
-    printf("Launch depth: %d\n", pb_choose_launch_depth(ctx, &root));
+    printf("Launch depth: %d\n", pb_prepare(ctx, &root, max_depth));
     fflush(stdout);
     for (int d = 1; d <= max_depth; d++) {
         pb_u128 v;
