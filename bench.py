@@ -227,26 +227,24 @@ def main():
         eng.set_tuning(leaf_kernel=args.leaf_kernel)
 
     # shard: depth-2 subtrees round-robin over ranks (one rank: the whole root)
+    from perft_gpu_2026_b200 import dist as pdist
+
     if world > 1:
-        subs = depth2_subtrees(pg, root)
-        mine = subs[rank::world]
+        mine = pdist.shard(pdist.subtrees(root, 2), world, rank)
         sub_depth = depth - 2
     else:
         mine = [root]
         sub_depth = depth
 
+    def run_once():
+        if len(mine) == 1:
+            return eng.perft_position(mine[0], sub_depth)
+        return sum(eng.perft_batch(mine, [sub_depth] * len(mine)))
+
     def step():
-        total, dev_ms, leaf_ms, leaf_pos, kernels, h2d, d2h = 0, 0.0, 0.0, 0, 0, 0, 0
-        for p in mine:
-            total += eng.perft_position(p, sub_depth)
-            st = eng.last_stats()
-            dev_ms += st.device_ms
-            leaf_ms += st.leaf_ms
-            leaf_pos += st.leaf_positions
-            kernels += st.kernels
-            h2d += st.h2d_bytes
-            d2h += st.d2h_bytes
-        return total, dev_ms, leaf_ms, leaf_pos, kernels, h2d, d2h
+        total = run_once()
+        st = eng.last_stats()
+        return total, st.device_ms, st.leaf_ms, st.leaf_positions, st.kernels, st.h2d_bytes, st.d2h_bytes
 
     for _ in range(args.warmup):
         step()
@@ -276,8 +274,7 @@ def main():
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
-        for p in mine:
-            eng.perft_position(p, sub_depth)
+        run_once()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     my_e2e = statistics.median(e2e_ms)
 

@@ -556,6 +556,227 @@ int gpu_perft(pb_ctx *ctx, const Board &b, u32 st, int c, int depth, u64 *out)
     return PB_OK;
 }
 
+// ---------------------------------------------------------------- batched roots
+// Colour normalisation: a position with black to move becomes its mirror
+// image with white to move (ranks reversed, colours swapped, castle rights
+// swapped); perft is unchanged.
+inline void to_white_to_move(const pb_pos &p, Board &b, uint8_t &st)
+{
+    b = to_board(p);
+    st = p.state;
+    if (p.color == WHITE) return;
+    u64 occ = b.bb[1] | b.bb[2] | b.bb[3];
+    u64 white = occ & ~b.bb[0];
+    b.bb[0] = __builtin_bswap64(white);
+    for (int k = 1; k < 4; k++) b.bb[k] = __builtin_bswap64(b.bb[k]);
+    st = (uint8_t)((st & 0xF0) | ((st & 3) << 2) | ((st >> 2) & 3));
+}
+
+// Batched breadth-first perft of n white-to-move roots at one depth;
+// out[i] = perft(depth) of root i.  BFS_TOO_BIG when a level does not fit.
+int bfs_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth, u64 *out, int *bfs_status)
+{
+    *bfs_status = BFS_OK;
+    const bool strict = ctx->opts.strict != 0;
+    if (n == 0) return PB_OK;
+    if (depth == 0) {
+        for (u64 i = 0; i < n; i++) out[i] = 1;
+        return PB_OK;
+    }
+    cudaStream_t s = ctx->stream;
+    pb_stats &stats = ctx->stats;
+    Arena ar{ctx->arena, ctx->arena_bytes};
+    Board *b0 = ar.take<Board>(n);
+    uint8_t *s0 = ar.take<uint8_t>(n);
+    u32 *r0 = ar.take<u32>(n);
+    u32 *cnt0 = ar.take<u32>(n);
+    u64 *off0 = ar.take<u64>(n);
+    unsigned long long *rc = ar.take<unsigned long long>(n);
+    u64 tiles0 = (n + SCAN_TILE - 1) / SCAN_TILE;
+    u64 *status0 = ar.take<u64>(tiles0);
+    if (!b0 || !s0 || !r0 || !cnt0 || !off0 || !rc || !status0) {
+        *bfs_status = BFS_TOO_BIG;
+        return PB_OK;
+    }
+    std::vector<u32> iota(n);
+    for (u64 i = 0; i < n; i++) iota[i] = (u32)i;
+    PB_CUDA(cudaMemcpyAsync(b0, rb, sizeof(Board) * n, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(s0, rs, n, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(r0, iota.data(), sizeof(u32) * n, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemsetAsync(rc, 0, sizeof(unsigned long long) * n, s));
+    PB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s));
+    PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(unsigned long long), s));
+    stats.h2d_bytes += (sizeof(Board) + 1 + 4) * n;
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[0], s));
+    if (depth == 1) {
+        if (strict)
+            k_count_positions<WHITE, true><<<grid_for(n, 256), 256, 0, s>>>(b0, s0, n, cnt0);
+        else
+            k_count_positions<WHITE, false><<<grid_for(n, 256), 256, 0, s>>>(b0, s0, n, cnt0);
+        PB_CUDA(cudaGetLastError());
+        std::vector<u32> tmp(n);
+        PB_CUDA(cudaMemcpyAsync(tmp.data(), cnt0, sizeof(u32) * n, cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+        for (u64 i = 0; i < n; i++) out[i] = tmp[i];
+        stats.kernels += 1;
+        stats.d2h_bytes += 4 * n;
+        return PB_OK;
+    }
+    // root moves as the first edges
+    k_count_positions<WHITE, true><<<grid_for(n, 256), 256, 0, s>>>(b0, s0, n, cnt0);
+    PB_CUDA(cudaMemsetAsync(status0, 0, sizeof(u64) * tiles0, s));
+    PB_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s));
+    k_scan<<<(unsigned)tiles0, SCAN_THREADS, 0, s>>>(cnt0, n, off0, status0, ctx->d_ticket, ctx->d_total, ctx->d_err);
+    PB_CUDA(cudaGetLastError());
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_total, sizeof(u64), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    stats.kernels += 2;
+    u64 ne = ctx->h_pinned[0];
+    if (ne > 0xFFFFFFFFULL) {
+        *bfs_status = BFS_TOO_BIG;
+        return PB_OK;
+    }
+    uint16_t *emv = ar.take<uint16_t>(ne ? ne : 1);
+    u32 *epi = ar.take<u32>(ne ? ne : 1);
+    if (!emv || !epi) {
+        *bfs_status = BFS_TOO_BIG;
+        return PB_OK;
+    }
+    if (ne) {
+        k_generate<WHITE><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(b0, s0, off0, ctx->d_total, n, emv, epi,
+                                                                         ctx->d_err);
+        PB_CUDA(cudaGetLastError());
+        stats.kernels += 1;
+    }
+    if (stats.levels < 16) stats.level_sizes[stats.levels] = ne;
+    Board *cur_b = b0;
+    uint8_t *cur_s = s0;
+    u32 *cur_r = r0;
+    u64 n_par = n;
+    int c = WHITE;
+    for (int rem = depth - 1; rem > 2 && ne; rem--) {
+        Board *cb = ar.take<Board>(ne);
+        uint8_t *cs = ar.take<uint8_t>(ne);
+        u32 *cr = ar.take<u32>(ne);
+        u32 *cnt = ar.take<u32>(ne);
+        u64 *offs = ar.take<u64>(ne);
+        u64 tiles = (ne + SCAN_TILE - 1) / SCAN_TILE;
+        u64 *status = ar.take<u64>(tiles);
+        if (!cb || !cs || !cr || !cnt || !offs || !status) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        unsigned g = grid_for(ne, 256);
+        if (c == WHITE)
+            k_expand_count_rooted<WHITE><<<g, 256, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, cb, cs, cr, cnt, ctx->d_err);
+        else
+            k_expand_count_rooted<BLACK><<<g, 256, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, cb, cs, cr, cnt, ctx->d_err);
+        PB_CUDA(cudaMemsetAsync(status, 0, sizeof(u64) * tiles, s));
+        PB_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s));
+        k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(cnt, ne, offs, status, ctx->d_ticket, ctx->d_total, ctx->d_err);
+        PB_CUDA(cudaGetLastError());
+        PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_total, sizeof(u64), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 1, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+        stats.kernels += 2;
+        stats.d2h_bytes += 12;
+        if ((u32)ctx->h_pinned[1]) return fail(ctx, PB_ERR_DEVICE, "batched level reported a device error");
+        u64 next = ctx->h_pinned[0];
+        stats.levels++;
+        if (stats.levels < 16) stats.level_sizes[stats.levels] = next;
+        cur_b = cb;
+        cur_s = cs;
+        cur_r = cr;
+        n_par = ne;
+        c = 1 - c;
+        if (next > 0xFFFFFFFFULL) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        uint16_t *nmv = ar.take<uint16_t>(next ? next : 1);
+        u32 *npi = ar.take<u32>(next ? next : 1);
+        if (!nmv || !npi) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        if (next) {
+            if (c == WHITE)
+                k_generate<WHITE><<<grid_for(n_par, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n_par, nmv, npi, ctx->d_err);
+            else
+                k_generate<BLACK><<<grid_for(n_par, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n_par, nmv, npi, ctx->d_err);
+            PB_CUDA(cudaGetLastError());
+            stats.kernels += 1;
+        }
+        emv = nmv;
+        epi = npi;
+        ne = next;
+    }
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[1], s));
+    if (ne) {
+        if (depth == 2) {
+            unsigned g = grid_for(ne, 256);
+            if (c == WHITE) {
+                if (strict) k_leaf1_rooted<WHITE, true><<<g, 256, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc);
+                else k_leaf1_rooted<WHITE, false><<<g, 256, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc);
+            } else {
+                if (strict) k_leaf1_rooted<BLACK, true><<<g, 256, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc);
+                else k_leaf1_rooted<BLACK, false><<<g, 256, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc);
+            }
+        } else {
+            unsigned g = grid_for(ne, PB_LEAF_THREADS);
+            if (c == WHITE) {
+                if (strict) k_leaf2_rooted<WHITE, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, ctx->d_counter);
+                else k_leaf2_rooted<WHITE, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, ctx->d_counter);
+            } else {
+                if (strict) k_leaf2_rooted<BLACK, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, ctx->d_counter);
+                else k_leaf2_rooted<BLACK, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, ctx->d_counter);
+            }
+        }
+        PB_CUDA(cudaGetLastError());
+        stats.kernels += 1;
+    }
+    if (ctx->timing) {
+        PB_CUDA(cudaEventRecord(ctx->ev[2], s));
+        PB_CUDA(cudaEventRecord(ctx->ev[3], s));
+    }
+    std::vector<unsigned long long> tmp(n);
+    PB_CUDA(cudaMemcpyAsync(tmp.data(), rc, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_counter, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 2, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    if ((u32)ctx->h_pinned[2]) return fail(ctx, PB_ERR_DEVICE, "batched leaf reported a device error");
+    for (u64 i = 0; i < n; i++) out[i] = tmp[i];
+    stats.leaf_edges += ne;
+    stats.leaf_positions += ctx->h_pinned[1];
+    stats.d2h_bytes += 8 * n + 20;
+    if (ctx->timing) {
+        float a = 0, b2 = 0;
+        PB_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[3]));
+        PB_CUDA(cudaEventElapsedTime(&b2, ctx->ev[1], ctx->ev[2]));
+        stats.device_ms += a;
+        stats.leaf_ms += b2;
+    }
+    return PB_OK;
+}
+
+// Batched perft with automatic halving when a level does not fit.
+int gpu_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth, u64 *out)
+{
+    int status = BFS_OK;
+    int rc = bfs_batch(ctx, rb, rs, n, depth, out, &status);
+    if (rc != PB_OK || status == BFS_OK) return rc;
+    if (n == 1) {
+        // one root too big for a batched pass: the single-root path splits it
+        pb_pos p;
+        to_pos(rb[0], rs[0], WHITE, p);
+        return gpu_perft(ctx, rb[0], rs[0], WHITE, depth, out);
+    }
+    u64 h = n / 2;
+    rc = gpu_batch(ctx, rb, rs, h, depth, out);
+    if (rc != PB_OK) return rc;
+    return gpu_batch(ctx, rb + h, rs + h, n - h, depth, out + h);
+}
+
 // ---------------------------------------------------------------- 128-bit helpers
 inline void add128(pb_u128 &a, const pb_u128 &b)
 {
@@ -920,9 +1141,26 @@ int pb_perft_batch(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, u
     if (!ctx || !roots || !depths || !counts || n < 0) return PB_ERR_ARG;
     if (!ctx->gpu) return fail(ctx, PB_ERR_NODEVICE, "context has no GPU");
     PB_CUDA(cudaSetDevice(ctx->device));
-    for (int i = 0; i < n; i++) {
-        int rc = gpu_perft(ctx, to_board(roots[i]), roots[i].state, roots[i].color, depths[i], reinterpret_cast<u64 *>(&counts[i]));
+    memset(&ctx->stats, 0, sizeof(ctx->stats));
+    // one batched pass per distinct depth
+    std::vector<int> ds(depths, depths + n);
+    std::sort(ds.begin(), ds.end());
+    ds.erase(std::unique(ds.begin(), ds.end()), ds.end());
+    for (int d : ds) {
+        if (d < 0 || d > 20) return PB_ERR_ARG;
+        std::vector<int> idx;
+        for (int i = 0; i < n; i++)
+            if (depths[i] == d) idx.push_back(i);
+        std::vector<Board> rb(idx.size());
+        std::vector<uint8_t> rs(idx.size());
+        for (size_t k = 0; k < idx.size(); k++) to_white_to_move(roots[idx[k]], rb[k], rs[k]);
+        std::vector<u64> out(idx.size());
+        int rc = gpu_batch(ctx, rb.data(), rs.data(), idx.size(), d, out.data());
         if (rc != PB_OK) return rc;
+        for (size_t k = 0; k < idx.size(); k++) {
+            counts[idx[k]] = out[k];
+            ctx->stats.nodes += out[k];
+        }
     }
     return PB_OK;
 }

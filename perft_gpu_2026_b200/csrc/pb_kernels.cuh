@@ -451,3 +451,119 @@ __global__ void __launch_bounds__(LEAF_T, 4) k_leaf2_coop(const Board *__restric
 }
 
 }  // namespace pb
+
+namespace pb {
+
+// ---------------------------------------------------------------- batched roots
+// Batched BFS over many roots at once.  Roots are normalised on the host so
+// that every root has white to move (a colour-flipped, rank-mirrored position
+// has the same perft), which keeps each level one colour.  Every position
+// carries the index of its root; the leaves add their counts to that root's
+// counter, aggregating lanes of a warp that share a root first.
+
+// Move count of each position (strict = sizing for the next level).
+template <int C, bool STRICT>
+__global__ void __launch_bounds__(256) k_count_positions(const Board *__restrict__ boards,
+                                                         const uint8_t *__restrict__ states, u64 n,
+                                                         u32 *__restrict__ counts)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    counts[i] = count_moves<C, STRICT>(load_board(boards + i), states[i]);
+}
+
+template <int C>
+__global__ void __launch_bounds__(256) k_expand_count_rooted(const Board *__restrict__ pboards,
+                                                             const uint8_t *__restrict__ pstates,
+                                                             const u32 *__restrict__ proot,
+                                                             const u32 *__restrict__ pidx,
+                                                             const uint16_t *__restrict__ moves, u64 n,
+                                                             u64 nparents, Board *__restrict__ cboards,
+                                                             uint8_t *__restrict__ cstates, u32 *__restrict__ croot,
+                                                             u32 *__restrict__ counts, u32 *__restrict__ err)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    u32 p = pidx[i];
+    if (p >= nparents) {
+        atomicOr(err, DEVERR_CAPACITY);
+        counts[i] = 0;
+        croot[i] = 0;
+        return;
+    }
+    Board b = load_board(pboards + p);
+    u32 st = pstates[p];
+    make_move<C>(b, st, moves[i]);
+    store_board(cboards + i, b);
+    cstates[i] = (uint8_t)st;
+    croot[i] = proot[p];
+    counts[i] = count_moves<1 - C, true>(b, st);
+}
+
+// Adds v to out[key] once per group of lanes holding the same key (edges of
+// one root are contiguous, so a warp usually forms one or two groups).
+__device__ __forceinline__ void add_by_key(unsigned long long *out, u32 key, u32 v, bool valid)
+{
+    const unsigned active = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    const unsigned peers = __match_any_sync(active, key);
+    const u32 total = __reduce_add_sync(peers, v);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1 && total) atomicAdd(out + key, (unsigned long long)total);
+}
+
+// Two-ply leaf over edges, counts credited to each edge's root.
+template <int C, bool STRICT>
+__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
+    k_leaf2_rooted(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                   const u32 *__restrict__ proot, const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
+                   u64 n, u64 nparents, unsigned long long *__restrict__ root_counts,
+                   unsigned long long *__restrict__ counter)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    u32 total = 0, counted = 0, root = 0;
+    bool valid = i < n && pidx[i] < nparents;
+    if (valid) {
+        u32 p = pidx[i];
+        root = proot[p];
+        Board b = load_board(pboards + p);
+        u32 st = pstates[p];
+        make_move<C>(b, st, moves[i]);
+        uint16_t mv[MAX_MOVES];
+        ArraySink sink{mv, 0};
+        gen_moves<1 - C>(b, st, sink);
+        for (int k = 0; k < sink.n; k++) {
+            Board g = b;
+            u32 gs = st;
+            make_move<1 - C>(g, gs, mv[k]);
+            total += count_moves<C, STRICT>(g, gs);
+        }
+        counted = sink.n;
+    }
+    add_by_key(root_counts, root, total, valid);
+    counted = __reduce_add_sync(0xffffffffu, counted);
+    if ((threadIdx.x & 31) == 0 && counted) atomicAdd(counter + 1, (unsigned long long)counted);
+}
+
+// One-ply leaf over edges (perft 1 of each edge's child), per root.
+template <int C, bool STRICT>
+__global__ void __launch_bounds__(256) k_leaf1_rooted(const Board *__restrict__ pboards,
+                                                      const uint8_t *__restrict__ pstates,
+                                                      const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
+                                                      const uint16_t *__restrict__ moves, u64 n, u64 nparents,
+                                                      unsigned long long *__restrict__ root_counts)
+{
+    u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    u32 cnt = 0, root = 0;
+    bool valid = i < n && pidx[i] < nparents;
+    if (valid) {
+        u32 p = pidx[i];
+        root = proot[p];
+        Board b = load_board(pboards + p);
+        u32 st = pstates[p];
+        make_move<C>(b, st, moves[i]);
+        cnt = count_moves<1 - C, STRICT>(b, st);
+    }
+    add_by_key(root_counts, root, cnt, valid);
+}
+
+}  // namespace pb

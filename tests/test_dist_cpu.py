@@ -1,0 +1,68 @@
+"""The multi-GPU sharding logic, run as two gloo ranks on CPU: every rank
+counts its subtrees with the host engine and one all-reduce gives the total,
+which must equal the single-process count."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+import perft_gpu_2026_b200 as pg
+from perft_gpu_2026_b200 import dist as pdist
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, fen, depth, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    eng = pg.Engine(device=-1)
+    root = pg.parse_fen(fen)
+
+    def count(positions, d):
+        return sum(eng.perft_cpu(p, d) for p in positions)
+
+    part = pdist.perft_sharded(root, depth, count, world, rank)
+    total = pdist.all_reduce_count(part)
+    q.put((rank, part, total))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("fen,depth", [(pg.START_FEN, 4), ("r3k2r/p1ppqpb1/bn2pnp1/3PN3/1p2P3/2N2Q1p/PPPBBPPP/R3K2R w KQkq -", 3)])
+def test_two_rank_gloo_perft(fen, depth):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, fen, depth, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    want = pg.Engine(device=-1).perft_cpu(pg.parse_fen(fen), depth)
+    assert all(total == want for _, _, total in res)
+    assert sum(part for _, part, _ in res) == want
+    assert all(part > 0 for _, part, _ in res)
+
+
+def test_shard_covers_every_subtree_once():
+    root = pg.parse_fen(pg.START_FEN)
+    subs = pdist.subtrees(root, 2)
+    assert len(subs) == 400
+    parts = [pdist.shard(subs, 3, r) for r in range(3)]
+    assert sum(len(p) for p in parts) == 400
+    keys = sorted(s.key() for p in parts for s in p)
+    assert keys == sorted(s.key() for s in subs)

@@ -149,3 +149,26 @@ def test_cli_gpu_output():
     lines = [l.split(",")[0] for l in out.splitlines() if l.startswith("Perft(")]
     assert lines == ["Perft(01): 48", "Perft(02): 2039", "Perft(03): 97862", "Perft(04): 4085603",
                      "Perft(05): 193690690"]
+
+
+def test_batch_matches_single_root_runs():
+    """Config-3 style roots (uneven playouts, both sides to move): one
+    batched pass per depth equals per-root plain runs, bit for bit."""
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=4 << 30)
+    roots = pg.uneven_roots(256, 6, 40, seed=2)
+    assert {r.color for r in roots} == {0, 1}
+    depths = [1 + (i % 5) for i in range(len(roots))]
+    got = eng.perft_batch(roots, depths)
+    want = [eng.perft_position(r, d) for r, d in zip(roots, depths)]
+    assert got == want
+    eng.close()
+
+
+def test_batch_splits_when_arena_is_small():
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=8 << 20)
+    roots = pg.uneven_roots(64, 6, 40, seed=7)
+    got = eng.perft_batch(roots, [5] * len(roots))
+    ref = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30)
+    assert got == [ref.perft_position(r, 5) for r in roots]
+    eng.close()
+    ref.close()
