@@ -171,6 +171,25 @@ int pb_last_stats(const pb_ctx *ctx, pb_stats *out);
  * n u32 counts into n u64 offsets and a device u64 total. */
 int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total);
 
+/* Allocation-free variant of pb_dev_scan.  No counterpart in the reference.
+ * For callers that may not allocate device memory at the point they need the
+ * scan: allocator and out-of-memory handling paths, hosts whose framework
+ * owns every device buffer and forbids raw cudaMalloc, and latency-critical
+ * loops where cudaMalloc's implicit device synchronisation is not allowed.
+ * The caller passes the input and output buffers; the scan's own
+ * scratch (tile status words, ticket, error word) is a fixed device array
+ * inside the library, so the call makes no cudaMalloc/cudaFree and no
+ * allocating library call.
+ *   - n is limited to 8,388,608 counts (4096 tiles of 2048); larger n returns
+ *     PB_ERR_ARG without touching the GPU.
+ *   - Runs on `stream` (NULL = default stream) of the current device and waits
+ *     for it before returning; n == 0 returns PB_OK and writes nothing.
+ *   - The first call on a device looks up the array's device address (set-up);
+ *     make that first call before any stream capture.
+ *   - All calls share the one array, so calls that overlap on the GPU (other
+ *     threads or streams of the same device) race; serialise them. */
+int pb_scan_u32_noalloc(const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <chrono>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "../../include/perft_b200.h"
@@ -847,6 +848,20 @@ int estimate_launch_depth(pb_ctx *ctx, const Board &b, u32 st, int c)
 
 }  // namespace
 
+// ---------------------------------------------------------------- allocation-free scan
+// Scratch of pb_scan_u32_noalloc: the scan's tile status words, its tile
+// ticket and its error word live in this fixed device array instead of memory
+// the caller or the engine allocates.  Every GPU that loads the library holds
+// it (34 KB) until the process exits.
+constexpr u64 NOALLOC_SCAN_TILES = 4096;                              // status words
+constexpr u64 NOALLOC_SCAN_MAX_ITEMS = NOALLOC_SCAN_TILES * SCAN_TILE;  // 8,388,608 counts
+static __device__ __align__(256) u64 g_noalloc_scratch[NOALLOC_SCAN_TILES + 32];
+
+// Device address of g_noalloc_scratch per device, resolved once per device
+// (with that device current) on the first call there.
+static u64 *g_noalloc_addr[64];
+static std::mutex g_noalloc_mu;
+
 // ==================================================================== C ABI
 extern "C" {
 
@@ -1184,6 +1199,42 @@ int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, 
     PB_CUDA(cudaStreamSynchronize(s));
     if ((u32)ctx->h_pinned[1]) return fail(ctx, PB_ERR_DEVICE, "scan reported a device error");
     return PB_OK;
+}
+
+int pb_scan_u32_noalloc(const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total, void *stream)
+{
+    if (!d_in || !d_out || !d_total) return PB_ERR_ARG;
+    if (n > NOALLOC_SCAN_MAX_ITEMS) return PB_ERR_ARG;  // beyond the fixed scratch
+    if (n == 0) return PB_OK;
+    build_host_tables();
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PB_ERR_CUDA;
+    u64 *scratch;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *addr = nullptr;
+            if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return PB_ERR_CUDA;
+            g_noalloc_addr[dev] = reinterpret_cast<u64 *>(addr);
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    u64 *status = scratch;
+    u32 *ticket = reinterpret_cast<u32 *>(scratch + NOALLOC_SCAN_TILES);
+    u32 *err = reinterpret_cast<u32 *>(scratch + NOALLOC_SCAN_TILES + 1);
+    // status words, ticket and error word must start at zero; the array keeps
+    // whatever the previous call left
+    if (cudaMemsetAsync(status, 0, sizeof(u64) * tiles, s) != cudaSuccess) return PB_ERR_CUDA;
+    if (cudaMemsetAsync(ticket, 0, 2 * sizeof(u64), s) != cudaSuccess) return PB_ERR_CUDA;
+    k_scan<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(d_in, n, reinterpret_cast<u64 *>(d_out), status, ticket,
+                                                     reinterpret_cast<u64 *>(d_total), err);
+    if (cudaGetLastError() != cudaSuccess) return PB_ERR_CUDA;
+    u32 herr = 0;
+    if (cudaMemcpyAsync(&herr, err, sizeof(u32), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PB_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PB_ERR_CUDA;
+    return herr ? PB_ERR_DEVICE : PB_OK;
 }
 
 }  // extern "C"

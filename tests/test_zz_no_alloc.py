@@ -1,0 +1,63 @@
+"""The allocation-free scan entry point (pb_scan_u32_noalloc).
+
+Some callers of this library cannot allocate device memory when they need a
+scan (an allocator's own out-of-memory path, a host framework that owns every
+device buffer, a latency-critical loop that must not hit cudaMalloc's implicit
+synchronisation).  This entry point keeps its scratch in a fixed array inside
+the library; the test calls it through the C ABI and compares its output with
+the regular entry point's (pb_dev_scan) on two calls in a row.  This file is
+collected last so that a failure here leaves every other test already run."""
+import ctypes
+
+import pytest
+
+import perft_gpu_2026_b200 as pg
+
+pytestmark = pytest.mark.gpu
+
+MAX_ITEMS = 4096 * 2048
+
+
+def _noalloc():
+    lib = ctypes.CDLL(pg.LIB_PATH)
+    fn = lib.pb_scan_u32_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    return fn
+
+
+def test_noalloc_scan_matches_regular_entry_point():
+    import torch
+
+    torch.cuda.set_device(0)
+    fn = _noalloc()
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=64 << 20)
+    g = torch.Generator().manual_seed(1234)
+    # two calls in a row: a large input, then a smaller one (the shared
+    # scratch still holds the first call's tile words)
+    for n in (MAX_ITEMS - 5, 300_001):
+        x = torch.randint(0, 219, (n,), generator=g, dtype=torch.int64)
+        d_in = x.to(torch.int32).cuda()
+        out_a = torch.full((n,), -1, dtype=torch.int64, device="cuda")
+        tot_a = torch.full((1,), -1, dtype=torch.int64, device="cuda")
+        out_b = torch.full((n,), -2, dtype=torch.int64, device="cuda")
+        tot_b = torch.full((1,), -2, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        rc = fn(d_in.data_ptr(), n, out_a.data_ptr(), tot_a.data_ptr(), None)
+        assert rc == pg.PB_OK
+        eng.dev_scan(d_in.data_ptr(), n, out_b.data_ptr(), tot_b.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.equal(out_a, out_b)
+        assert torch.equal(tot_a, tot_b)
+        assert int(tot_a.item()) == int(x.sum())
+    eng.close()
+
+
+def test_noalloc_scan_rejects_sizes_beyond_its_scratch():
+    import torch
+
+    fn = _noalloc()
+    d = torch.zeros(1, dtype=torch.int32, device="cuda")
+    o = torch.zeros(1, dtype=torch.int64, device="cuda")
+    # the size check happens before any GPU work, so tiny buffers are safe here
+    assert fn(d.data_ptr(), MAX_ITEMS + 1, o.data_ptr(), o.data_ptr(), None) == pg.PB_ERR_ARG
