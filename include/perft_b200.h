@@ -171,6 +171,38 @@ int pb_last_stats(const pb_ctx *ctx, pb_stats *out);
  * n u32 counts into n u64 offsets and a device u64 total. */
 int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total);
 
+/* Learned scheduler network (no reference counterpart): 781 binary inputs
+ * (12x64 piece-square, side to move, 4 castle rights, 8 en-passant files) ->
+ * 256 -> 256 -> 4 outputs = predicted log2(1 + perft(k)), k = 1..4.  BF16
+ * weights with an FP32 master copy, FP32 accumulation, Adam; trained and run
+ * by the library's own kernels on the context's GPU.  Parameter layout of
+ * get/set: [W1 781x256 | b1 256 | W2 256x256 | b2 256 | W3 256x4 | b3 4]. */
+size_t pb_mlp_param_count(void);
+int pb_mlp_init(pb_ctx *ctx, uint64_t seed, const float *out_bias);
+int pb_mlp_get_params(pb_ctx *ctx, float *out, size_t count);
+int pb_mlp_set_params(pb_ctx *ctx, const float *in, size_t count);
+/* Mean squared error and gradients of one batch (n a multiple of 64). */
+int pb_mlp_gradients(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n, float *grads, float *loss);
+int pb_mlp_train(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n, int epochs, int batch, float lr,
+                 uint64_t seed, float *final_loss);
+int pb_mlp_predict(pb_ctx *ctx, const pb_pos *pos, int n, float *out);
+
+/* Learned batch planner (no reference counterpart): like pb_perft_batch, but
+ * the network's predictions size every BFS level up front, bin-pack the roots
+ * into batches that fit the arena and split roots too large for one batch;
+ * each batch runs as one captured CUDA graph (device-side sizes, a persistent
+ * leaf fed by a device work queue).  A batch that outgrows its planned sizes
+ * is rerun with the exact count-then-allocate path; counts are exact either
+ * way.  Needs pb_mlp_init (and normally pb_mlp_train) first. */
+typedef struct {
+    uint32_t batches;        /* batches run */
+    uint32_t graph_batches;  /* of which as planned CUDA graphs */
+    uint32_t retries;        /* planned batches rerun with exact sizing */
+    uint32_t split_roots;    /* roots split into children for size */
+} pb_plan_stats;
+int pb_perft_batch_planned(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uint64_t *counts,
+                           pb_plan_stats *stats);
+
 /* Allocation-free variant of pb_dev_scan.  No counterpart in the reference.
  * For callers that may not allocate device memory at the point they need the
  * scan: allocator and out-of-memory handling paths, hosts whose framework

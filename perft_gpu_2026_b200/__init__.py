@@ -89,6 +89,11 @@ class Tuning(ctypes.Structure):
                 ("reserved", ctypes.c_int * 6)]
 
 
+class PlanStats(ctypes.Structure):
+    _fields_ = [("batches", ctypes.c_uint32), ("graph_batches", ctypes.c_uint32), ("retries", ctypes.c_uint32),
+                ("split_roots", ctypes.c_uint32)]
+
+
 class PerftError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"perft engine error {code}: {msg}")
@@ -124,6 +129,17 @@ def _load() -> ctypes.CDLL:
         "pb_set_tuning": (ctypes.c_int, [ctypes.c_void_p, P(Tuning)]),
         "pb_get_tuning": (ctypes.c_int, [ctypes.c_void_p, P(Tuning)]),
         "pb_last_stats": (ctypes.c_int, [ctypes.c_void_p, P(Stats)]),
+        "pb_mlp_param_count": (ctypes.c_size_t, []),
+        "pb_mlp_init": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, P(ctypes.c_float)]),
+        "pb_mlp_get_params": (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_float), ctypes.c_size_t]),
+        "pb_mlp_set_params": (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_float), ctypes.c_size_t]),
+        "pb_mlp_gradients": (ctypes.c_int, [ctypes.c_void_p, P(Pos), P(ctypes.c_float), ctypes.c_int,
+                                             P(ctypes.c_float), P(ctypes.c_float)]),
+        "pb_mlp_train": (ctypes.c_int, [ctypes.c_void_p, P(Pos), P(ctypes.c_float), ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_float, ctypes.c_uint64, P(ctypes.c_float)]),
+        "pb_mlp_predict": (ctypes.c_int, [ctypes.c_void_p, P(Pos), ctypes.c_int, P(ctypes.c_float)]),
+        "pb_perft_batch_planned": (ctypes.c_int, [ctypes.c_void_p, P(Pos), P(ctypes.c_int), ctypes.c_int,
+                                                   P(ctypes.c_uint64), P(PlanStats)]),
         "pb_dev_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
@@ -315,6 +331,16 @@ class Engine:
         self._check(lib.pb_perft_cpu(self._h, ctypes.byref(p), depth, ctypes.byref(out)))
         return out.value
 
+    def perft_batch_planned(self, roots: Sequence[Pos], depths: Sequence[int]):
+        """Learned-planner batch: returns (counts, PlanStats)."""
+        n = len(roots)
+        arr = (Pos * n)(*roots)
+        d = (ctypes.c_int * n)(*depths)
+        out = (ctypes.c_uint64 * n)()
+        st = PlanStats()
+        self._check(lib.pb_perft_batch_planned(self._h, arr, d, n, out, ctypes.byref(st)))
+        return list(out), st
+
     def perft_batch(self, roots: Sequence[Pos], depths: Sequence[int]) -> List[int]:
         n = len(roots)
         arr = (Pos * n)(*roots)
@@ -347,6 +373,59 @@ class Engine:
 
     def choose_launch_depth(self, p: Pos) -> int:
         return lib.pb_choose_launch_depth(self._h, ctypes.byref(p))
+
+    # ---- learned scheduler network
+    def mlp_init(self, seed: int = 1, out_bias=None) -> None:
+        ob = (ctypes.c_float * 4)(*out_bias) if out_bias is not None else None
+        self._check(lib.pb_mlp_init(self._h, seed, ob))
+
+    def mlp_params(self):
+        import numpy as np
+
+        n = lib.pb_mlp_param_count()
+        buf = np.empty(n, dtype=np.float32)
+        self._check(lib.pb_mlp_get_params(self._h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n))
+        return buf
+
+    def mlp_set_params(self, params) -> None:
+        import numpy as np
+
+        buf = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(lib.pb_mlp_set_params(self._h, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), buf.size))
+
+    def mlp_gradients(self, positions: Sequence[Pos], targets):
+        import numpy as np
+
+        n = len(positions)
+        arr = (Pos * n)(*positions)
+        t = np.ascontiguousarray(targets, dtype=np.float32).reshape(n, 4)
+        g = np.empty(lib.pb_mlp_param_count(), dtype=np.float32)
+        loss = ctypes.c_float()
+        FP = ctypes.POINTER(ctypes.c_float)
+        self._check(lib.pb_mlp_gradients(self._h, arr, t.ctypes.data_as(FP), n, g.ctypes.data_as(FP),
+                                         ctypes.byref(loss)))
+        return g, loss.value
+
+    def mlp_train(self, positions: Sequence[Pos], targets, epochs: int, batch: int = 4096, lr: float = 1e-3,
+                  seed: int = 7) -> float:
+        import numpy as np
+
+        n = len(positions)
+        arr = (Pos * n)(*positions)
+        t = np.ascontiguousarray(targets, dtype=np.float32).reshape(n, 4)
+        loss = ctypes.c_float()
+        self._check(lib.pb_mlp_train(self._h, arr, t.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, epochs,
+                                     batch, lr, seed, ctypes.byref(loss)))
+        return loss.value
+
+    def mlp_predict(self, positions: Sequence[Pos]):
+        import numpy as np
+
+        n = len(positions)
+        arr = (Pos * n)(*positions)
+        out = np.empty((n, 4), dtype=np.float32)
+        self._check(lib.pb_mlp_predict(self._h, arr, n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
 
     def dev_scan(self, d_in: int, n: int, d_out: int, d_total: int) -> None:
         self._check(lib.pb_dev_scan(self._h, ctypes.c_void_p(d_in), n, ctypes.c_void_p(d_out), ctypes.c_void_p(d_total)))

@@ -27,10 +27,32 @@
 #include "pb_kernels.cuh"
 #include "pb_tt.cuh"
 #include "pb_devtt.cuh"
+#include "pb_mlp_host.cuh"
 
 using namespace pb;
 
 #define PB_VERSION "perft-b200 0.1"
+
+namespace pb {
+struct GraphPlan {
+    u64 n = 0;
+    int depth = 0;
+    bool strict = false;
+    std::vector<u64> caps;
+    cudaGraphExec_t exec = nullptr;
+    // device buffers inside the arena (fixed for the captured graph)
+    Board *b0 = nullptr;
+    uint8_t *s0 = nullptr;
+    u32 *r0 = nullptr;
+    unsigned long long *rc = nullptr;
+    u64 *sizes = nullptr;
+    bool same(u64 n_, int d_, bool s_, const std::vector<u64> &c_) const
+    {
+        return exec && n == n_ && depth == d_ && strict == s_ && caps == c_;
+    }
+};
+
+}  // namespace pb
 
 struct pb_ctx {
     int device = -1;
@@ -55,6 +77,8 @@ struct pb_ctx {
     pb_stats stats{};
     HostTT htt;
     DeviceTT dtt;
+    Mlp mlp;
+    GraphPlan graph;
     int dtt_max_depth = 0;
     size_t dtt_free_bytes = 0;
     u32 dedup_gen = 0;
@@ -778,6 +802,352 @@ int gpu_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth,
     return gpu_batch(ctx, rb + h, rs + h, n - h, depth, out + h);
 }
 
+// ---------------------------------------------------------------- planned batches (CUDA graph)
+// A batch whose level sizes were planned ahead (from the learned size
+// predictions) runs as one captured CUDA graph: every level's kernels read
+// their sizes from device memory, the leaf is a persistent kernel fed by a
+// device work queue, and nothing returns to the host until the root counts
+// do.  caps[k] bounds the edges of level k+1 (k = 0: root moves).
+struct GraphLevel {
+    Board *b;
+    uint8_t *s;
+    u32 *r, *cnt;
+    u64 *off, *status;
+    uint16_t *mv;
+    u32 *pi;
+    u64 tiles;
+};
+
+template <int C, bool S>
+void launch_leaf_queue(cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r, const u32 *pi,
+                       const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev, u64 npar_cap,
+                       unsigned long long *cursor, unsigned long long *rc, unsigned long long *counter, u32 *err)
+{
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf2_rooted_queue<C, S>, PB_LEAF_THREADS, 0);
+    if (per_sm <= 0) per_sm = 1;
+    unsigned grid = (unsigned)std::min<u64>((u64)sms * per_sm, (cap + PB_LEAF_THREADS - 1) / PB_LEAF_THREADS + 1);
+    k_leaf2_rooted_queue<C, S><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap,
+                                                                cursor, rc, counter, err);
+}
+
+// Builds (captures) the graph for a planned batch shape.
+int capture_batch_graph(pb_ctx *ctx, GraphPlan &g)
+{
+    cudaStream_t s = ctx->stream;
+    const u64 n = g.n;
+    const int depth = g.depth;
+    Arena ar{ctx->arena, ctx->arena_bytes};
+    g.b0 = ar.take<Board>(n);
+    g.s0 = ar.take<uint8_t>(n);
+    g.r0 = ar.take<u32>(n);
+    g.rc = ar.take<unsigned long long>(n);
+    u32 *cnt0 = ar.take<u32>(n);
+    u64 *off0 = ar.take<u64>(n);
+    u64 tiles0 = (n + SCAN_TILE - 1) / SCAN_TILE;
+    u64 *status0 = ar.take<u64>(tiles0);
+    const int nlev = std::max(depth - 2, 1);  // edge levels E_1 .. E_nlev
+    g.sizes = ar.take<u64>(nlev + 4);
+    unsigned long long *cursor = ar.take<unsigned long long>(1);
+    if (!g.b0 || !g.s0 || !g.r0 || !g.rc || !cnt0 || !off0 || !status0 || !g.sizes || !cursor) return PB_ERR_NOMEM;
+    std::vector<GraphLevel> L(nlev + 1);
+    for (int k = 1; k <= nlev; k++) {
+        u64 cap = g.caps[k - 1];
+        L[k].mv = ar.take<uint16_t>(cap);
+        L[k].pi = ar.take<u32>(cap);
+        if (!L[k].mv || !L[k].pi) return PB_ERR_NOMEM;
+        if (k < nlev || depth == 2) {
+            // positions of level k (the children of E_k) are materialised
+            // for every level but the last (the leaf makes those itself)
+        }
+        if (k < nlev) {
+            L[k].b = ar.take<Board>(cap);
+            L[k].s = ar.take<uint8_t>(cap);
+            L[k].r = ar.take<u32>(cap);
+            L[k].cnt = ar.take<u32>(cap);
+            L[k].off = ar.take<u64>(cap);
+            L[k].tiles = (cap + SCAN_TILE - 1) / SCAN_TILE;
+            L[k].status = ar.take<u64>(L[k].tiles);
+            if (!L[k].b || !L[k].s || !L[k].r || !L[k].cnt || !L[k].off || !L[k].status) return PB_ERR_NOMEM;
+        }
+    }
+    u64 *d_n0 = g.sizes;  // [0] = roots, [k] = edges of level k
+    std::vector<u64> init(nlev + 4, 0);
+    init[0] = n;
+    PB_CUDA(cudaMemcpy(g.sizes, init.data(), sizeof(u64) * init.size(), cudaMemcpyHostToDevice));
+    {
+        std::vector<u32> iota(n);
+        for (u64 i = 0; i < n; i++) iota[i] = (u32)i;
+        PB_CUDA(cudaMemcpy(g.r0, iota.data(), sizeof(u32) * n, cudaMemcpyHostToDevice));
+    }
+    cudaGraph_t graph = nullptr;
+    PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(g.rc, 0, sizeof(unsigned long long) * n, s);
+    cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s);
+    cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s);
+    // level 0: root move counts -> E_1
+    k_count_positions<WHITE, true><<<grid_for(n, 256), 256, 0, s>>>(g.b0, g.s0, n, cnt0);
+    cudaMemsetAsync(status0, 0, sizeof(u64) * tiles0, s);
+    cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s);
+    k_scan_dev<<<(unsigned)tiles0, SCAN_THREADS, 0, s>>>(cnt0, d_n0, n, off0, status0, ctx->d_ticket, d_n0 + 1, ctx->d_err);
+    k_generate_dev<WHITE><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(g.b0, g.s0, off0, d_n0 + 1, d_n0, n,
+                                                                           g.caps[0], L[1].mv, L[1].pi, ctx->d_err);
+    // middle levels: E_k -> positions P_k -> E_{k+1}
+    const Board *pb_ = g.b0;
+    const uint8_t *ps = g.s0;
+    const u32 *pr = g.r0;
+    const u64 *npar = d_n0;
+    u64 npar_cap = n;
+    int c = WHITE;
+    for (int k = 1; k < nlev; k++) {
+        u64 cap = g.caps[k - 1];
+        unsigned ge = (unsigned)std::min<u64>((cap + 255) / 256, (u64)ctx->num_sms * 16);
+        if (c == WHITE)
+            k_expand_rooted_dev<WHITE><<<ge, 256, 0, s>>>(pb_, ps, pr, L[k].pi, L[k].mv, d_n0 + k, cap, npar, npar_cap,
+                                                          L[k].b, L[k].s, L[k].r, L[k].cnt, ctx->d_err);
+        else
+            k_expand_rooted_dev<BLACK><<<ge, 256, 0, s>>>(pb_, ps, pr, L[k].pi, L[k].mv, d_n0 + k, cap, npar, npar_cap,
+                                                          L[k].b, L[k].s, L[k].r, L[k].cnt, ctx->d_err);
+        c = 1 - c;
+        cudaMemsetAsync(L[k].status, 0, sizeof(u64) * L[k].tiles, s);
+        cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s);
+        k_scan_dev<<<(unsigned)L[k].tiles, SCAN_THREADS, 0, s>>>(L[k].cnt, d_n0 + k, cap, L[k].off, L[k].status,
+                                                                 ctx->d_ticket, d_n0 + k + 1, ctx->d_err);
+        if (c == WHITE)
+            k_generate_dev<WHITE><<<grid_for(cap, GEN_THREADS), GEN_THREADS, 0, s>>>(
+                L[k].b, L[k].s, L[k].off, d_n0 + k + 1, d_n0 + k, cap, g.caps[k], L[k + 1].mv, L[k + 1].pi, ctx->d_err);
+        else
+            k_generate_dev<BLACK><<<grid_for(cap, GEN_THREADS), GEN_THREADS, 0, s>>>(
+                L[k].b, L[k].s, L[k].off, d_n0 + k + 1, d_n0 + k, cap, g.caps[k], L[k + 1].mv, L[k + 1].pi, ctx->d_err);
+        pb_ = L[k].b;
+        ps = L[k].s;
+        pr = L[k].r;
+        npar = d_n0 + k;
+        npar_cap = cap;
+    }
+    // leaf over E_nlev
+    const u64 lcap = g.caps[nlev - 1];
+    if (depth == 2) {
+        unsigned gl = (unsigned)std::min<u64>((lcap + 255) / 256, (u64)ctx->num_sms * 16);
+        if (g.strict)
+            k_leaf1_rooted_dev<WHITE, true><<<gl, 256, 0, s>>>(pb_, ps, pr, L[1].pi, L[1].mv, d_n0 + 1, lcap, npar,
+                                                               npar_cap, g.rc, ctx->d_err);
+        else
+            k_leaf1_rooted_dev<WHITE, false><<<gl, 256, 0, s>>>(pb_, ps, pr, L[1].pi, L[1].mv, d_n0 + 1, lcap, npar,
+                                                                npar_cap, g.rc, ctx->d_err);
+    } else if (c == WHITE) {
+        if (g.strict)
+            launch_leaf_queue<WHITE, true>(s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
+                                           npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
+        else
+            launch_leaf_queue<WHITE, false>(s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
+                                            npar, npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
+    } else {
+        if (g.strict)
+            launch_leaf_queue<BLACK, true>(s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
+                                           npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
+        else
+            launch_leaf_queue<BLACK, false>(s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
+                                            npar, npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "end capture");
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    ce = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "graph instantiate");
+    return PB_OK;
+}
+
+// Runs one planned batch; *overflow = true when a level outgrew its planned
+// capacity (results then invalid: the caller reruns with exact sizing).
+int run_planned_batch(pb_ctx *ctx, GraphPlan &g, const Board *rb, const uint8_t *rs, u64 n, int depth,
+                      const std::vector<u64> &caps, u64 *out, bool *overflow)
+{
+    *overflow = false;
+    const bool strict = ctx->opts.strict != 0;
+    if (!g.same(n, depth, strict, caps)) {
+        g.n = n;
+        g.depth = depth;
+        g.strict = strict;
+        g.caps = caps;
+        int rc = capture_batch_graph(ctx, g);
+        if (rc != PB_OK) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+            return rc;
+        }
+    }
+    cudaStream_t s = ctx->stream;
+    PB_CUDA(cudaMemcpyAsync(g.b0, rb, sizeof(Board) * n, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(g.s0, rs, n, cudaMemcpyHostToDevice, s));
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[0], s));
+    PB_CUDA(cudaGraphLaunch(g.exec, s));
+    if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[3], s));
+    std::vector<unsigned long long> tmp(n);
+    PB_CUDA(cudaMemcpyAsync(tmp.data(), g.rc, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_counter, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 2, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    u32 err = (u32)ctx->h_pinned[2];
+    ctx->stats.kernels += 3 * (u32)std::max(depth - 3, 0) + 3 + 1;
+    ctx->stats.h2d_bytes += (sizeof(Board) + 1) * n;
+    ctx->stats.d2h_bytes += 8 * n + 20;
+    if (ctx->timing) {
+        float a = 0;
+        PB_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[3]));
+        ctx->stats.device_ms += a;
+    }
+    if (err & DEVERR_OVERFLOW) {
+        *overflow = true;
+        return PB_OK;
+    }
+    if (err) return fail(ctx, PB_ERR_DEVICE, "planned batch reported a device error");
+    for (u64 i = 0; i < n; i++) out[i] = tmp[i];
+    ctx->stats.leaf_positions += ctx->h_pinned[1];
+    return PB_OK;
+}
+
+// ---------------------------------------------------------------- learned planning
+// Level sizes of a depth-d batched perft of one root, from the network's
+// predicted log2(1 + perft(k)), k = 1..4 (geometric beyond 4).
+void predicted_levels(const float *y, int depth, std::vector<double> &e)
+{
+    e.assign(std::max(depth - 2, 1), 0.0);
+    double p[5] = {1, 0, 0, 0, 0};
+    for (int k = 1; k <= 4; k++) p[k] = std::max(exp2((double)y[k - 1]) - 1.0, 0.0);
+    double bf = p[3] > 0 ? std::max(p[4] / p[3], 1.0) : 30.0;
+    for (int k = 1; k <= (int)e.size(); k++) e[k - 1] = k <= 4 ? p[k] : e[k - 2] * bf;
+}
+
+// bytes one root's batched levels take: 6 B per edge, 50 B per materialised position
+double level_bytes(const std::vector<double> &e)
+{
+    double b = 0;
+    for (size_t k = 0; k < e.size(); k++) b += e[k] * (6.0 + (k + 1 < e.size() ? 50.0 : 0.0));
+    return b;
+}
+
+struct PlanItem {
+    Board b;
+    uint8_t s;
+    int depth;
+    int owner;
+    double bytes;
+    std::vector<double> lv;
+};
+
+}  // namespace
+namespace {
+
+// Learned batch planner: predictions size every level of a batch up front,
+// bin-pack roots into batches that fit the arena, and split roots too big
+// for one batch into their children (the per-root launch-depth choice).
+// Batches then run as captured graphs; a batch whose levels outgrow the plan
+// is rerun with exact count-then-allocate sizing (counted in plan stats).
+int plan_and_run(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uint64_t *counts, pb_plan_stats *ps)
+{
+    const double margin = 1.3;
+    const double budget = (double)ctx->arena_bytes * 0.45 / margin;
+    std::vector<PlanItem> items;
+    items.reserve(n);
+    for (int i = 0; i < n; i++) {
+        PlanItem it;
+        to_white_to_move(roots[i], it.b, it.s);
+        it.depth = depths[i];
+        it.owner = i;
+        it.bytes = 0;
+        items.push_back(it);
+        counts[i] = 0;
+    }
+    std::vector<PlanItem> ready;
+    int guard = 0;
+    while (!items.empty() && guard++ < 8) {
+        // predict
+        std::vector<pb_pos> pp(items.size());
+        for (size_t k = 0; k < items.size(); k++) to_pos(items[k].b, items[k].s, WHITE, pp[k]);
+        std::vector<float> y(items.size() * MLP_OUT);
+        int rc = pb_mlp_predict(ctx, pp.data(), (int)pp.size(), y.data());
+        if (rc != PB_OK) return rc;
+        std::vector<PlanItem> next;
+        for (size_t k = 0; k < items.size(); k++) {
+            PlanItem &it = items[k];
+            predicted_levels(&y[k * MLP_OUT], it.depth, it.lv);
+            it.bytes = level_bytes(it.lv);
+            if (it.depth >= 4 && it.bytes > budget) {
+                // too big for any batch: split into children one ply down
+                uint16_t mv[MAX_MOVES];
+                int m = host_gen(it.b, it.s, WHITE, mv);
+                for (int j = 0; j < m; j++) {
+                    PlanItem c;
+                    c.b = it.b;
+                    u32 st = it.s;
+                    host_make(c.b, st, WHITE, mv[j]);
+                    // child has black to move: mirror it back to white
+                    pb_pos cp;
+                    to_pos(c.b, st, BLACK, cp);
+                    to_white_to_move(cp, c.b, c.s);
+                    c.depth = it.depth - 1;
+                    c.owner = it.owner;
+                    c.bytes = 0;
+                    next.push_back(c);
+                }
+                if (ps) ps->split_roots++;
+            } else {
+                ready.push_back(it);
+            }
+        }
+        items.swap(next);
+    }
+    if (!items.empty()) return fail(ctx, PB_ERR_NOMEM, "planner could not fit a root");
+    // bin-pack per depth: largest first, fill to the budget
+    std::sort(ready.begin(), ready.end(), [](const PlanItem &a, const PlanItem &b) {
+        return a.depth != b.depth ? a.depth < b.depth : a.bytes > b.bytes;
+    });
+    size_t i = 0;
+    while (i < ready.size()) {
+        int d = ready[i].depth;
+        size_t j = i;
+        double used = 0;
+        while (j < ready.size() && ready[j].depth == d && (j == i || used + ready[j].bytes <= budget) &&
+               j - i < 0xFFFFFFF) {
+            used += ready[j].bytes;
+            j++;
+        }
+        u64 m = j - i;
+        std::vector<Board> rb(m);
+        std::vector<uint8_t> rs(m);
+        std::vector<u64> out(m, 0);
+        for (u64 k = 0; k < m; k++) {
+            rb[k] = ready[i + k].b;
+            rs[k] = ready[i + k].s;
+        }
+        int rc = PB_OK;
+        bool overflow = false;
+        if (d <= 1) {
+            rc = gpu_batch(ctx, rb.data(), rs.data(), m, d, out.data());
+        } else {
+            std::vector<u64> caps(std::max(d - 2, 1), 0);
+            for (u64 k = 0; k < m; k++)
+                for (size_t l = 0; l < caps.size(); l++) caps[l] += (u64)ready[i + k].lv[l];
+            for (auto &c : caps) c = (u64)((double)c * margin) + 4096;
+            rc = run_planned_batch(ctx, ctx->graph, rb.data(), rs.data(), m, d, caps, out.data(), &overflow);
+            if (rc == PB_OK && overflow) {
+                if (ps) ps->retries++;
+                rc = gpu_batch(ctx, rb.data(), rs.data(), m, d, out.data());
+            }
+            if (ps) ps->graph_batches++;
+        }
+        if (rc != PB_OK) return rc;
+        for (u64 k = 0; k < m; k++) counts[ready[i + k].owner] += out[k];
+        if (ps) ps->batches++;
+        i = j;
+    }
+    return PB_OK;
+}
+
 // ---------------------------------------------------------------- 128-bit helpers
 inline void add128(pb_u128 &a, const pb_u128 &b)
 {
@@ -941,6 +1311,8 @@ void pb_destroy(pb_ctx *ctx)
         cudaSetDevice(ctx->device);
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         ctx->dtt.release();
+        ctx->mlp.release();
+        if (ctx->graph.exec) cudaGraphExecDestroy(ctx->graph.exec);
         for (int i = 0; i < 4; i++)
             if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
         if (ctx->arena) cudaFree(ctx->arena);
@@ -1235,6 +1607,142 @@ int pb_scan_u32_noalloc(const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint6
     if (cudaMemcpyAsync(&herr, err, sizeof(u32), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PB_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return PB_ERR_CUDA;
     return herr ? PB_ERR_DEVICE : PB_OK;
+}
+
+// ---------------------------------------------------------------- learned scheduler network
+size_t pb_mlp_param_count(void) { return MLP_PARAMS; }
+
+int pb_mlp_init(pb_ctx *ctx, uint64_t seed, const float *out_bias)
+{
+    if (!ctx || !ctx->gpu) return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    PB_CUDA(ctx->mlp.init(seed, out_bias, ctx->stream));
+    PB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PB_OK;
+}
+
+int pb_mlp_get_params(pb_ctx *ctx, float *out, size_t count)
+{
+    if (!ctx || !ctx->mlp.ready || !out || count != MLP_PARAMS) return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    PB_CUDA(cudaMemcpyAsync(out, ctx->mlp.p, MLP_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    PB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PB_OK;
+}
+
+int pb_mlp_set_params(pb_ctx *ctx, const float *in, size_t count)
+{
+    if (!ctx || !ctx->mlp.ready || !in || count != MLP_PARAMS) return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    PB_CUDA(ctx->mlp.set_params(in, ctx->stream));
+    PB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return PB_OK;
+}
+
+// Loss and parameter gradients of one batch (n a multiple of 64), no update.
+int pb_mlp_gradients(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n, float *grads, float *loss)
+{
+    if (!ctx || !ctx->mlp.ready || !pos || !targets || n <= 0 || n % 64) return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    Mlp &m = ctx->mlp;
+    cudaStream_t s = ctx->stream;
+    PB_CUDA(m.alloc_batch(n));
+    PB_CUDA(m.load_positions(pos, n, s));
+    PB_CUDA(cudaMemcpyAsync(m.t, targets, sizeof(float) * MLP_OUT * n, cudaMemcpyHostToDevice, s));
+    PB_CUDA(m.forward_backward(n, true, s));
+    if (grads) PB_CUDA(cudaMemcpyAsync(grads, m.g, MLP_PARAMS * sizeof(float), cudaMemcpyDeviceToHost, s));
+    float l = 0;
+    PB_CUDA(cudaMemcpyAsync(&l, m.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    if (loss) *loss = l / (float)(n * MLP_OUT);
+    return PB_OK;
+}
+
+// Adam training on n examples: `epochs` passes over a fresh shuffle each, in
+// batches of `batch` (a multiple of 64; the tail that does not fill a batch
+// is left out of that epoch).  *final_loss = mean squared error of the last
+// epoch.
+int pb_mlp_train(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n, int epochs, int batch, float lr,
+                 uint64_t seed, float *final_loss)
+{
+    if (!ctx || !ctx->mlp.ready || !pos || !targets || n <= 0 || batch <= 0 || batch % 64 || epochs <= 0)
+        return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    Mlp &m = ctx->mlp;
+    cudaStream_t s = ctx->stream;
+    PB_CUDA(m.alloc_batch(batch));
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::vector<pb_pos> bp(batch);
+    std::vector<float> bt((size_t)batch * MLP_OUT);
+    u64 rng = seed;
+    double epoch_loss = 0;
+    for (int ep = 0; ep < epochs; ep++) {
+        for (int i = n - 1; i > 0; i--) {
+            u64 r = splitmix64(&rng);
+            int j = (int)(((unsigned __int128)r * (u64)(i + 1)) >> 64);
+            std::swap(order[i], order[j]);
+        }
+        epoch_loss = 0;
+        int steps = 0;
+        for (int b0 = 0; b0 + batch <= n; b0 += batch) {
+            for (int k = 0; k < batch; k++) {
+                bp[k] = pos[order[b0 + k]];
+                memcpy(&bt[(size_t)k * MLP_OUT], targets + (size_t)order[b0 + k] * MLP_OUT, sizeof(float) * MLP_OUT);
+            }
+            PB_CUDA(m.load_positions(bp.data(), batch, s));
+            PB_CUDA(cudaMemcpyAsync(m.t, bt.data(), sizeof(float) * bt.size(), cudaMemcpyHostToDevice, s));
+            PB_CUDA(m.forward_backward(batch, true, s));
+            PB_CUDA(m.adam_step(lr, s));
+            float l = 0;
+            PB_CUDA(cudaMemcpyAsync(&l, m.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+            PB_CUDA(cudaStreamSynchronize(s));
+            epoch_loss += l / (double)(batch * MLP_OUT);
+            steps++;
+        }
+        if (steps) epoch_loss /= steps;
+    }
+    if (final_loss) *final_loss = (float)epoch_loss;
+    return PB_OK;
+}
+
+// Predicted log2(1 + perft(k)), k = 1..4, for n positions (out: n x 4).
+int pb_mlp_predict(pb_ctx *ctx, const pb_pos *pos, int n, float *out)
+{
+    if (!ctx || !ctx->mlp.ready || !pos || !out || n < 0) return PB_ERR_ARG;
+    if (n == 0) return PB_OK;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    Mlp &m = ctx->mlp;
+    cudaStream_t s = ctx->stream;
+    const int chunk = 8192;
+    PB_CUDA(m.alloc_batch(chunk));
+    for (int b0 = 0; b0 < n; b0 += chunk) {
+        int k = std::min(chunk, n - b0);
+        int padded = (k + 63) / 64 * 64;
+        std::vector<pb_pos> tmp(pos + b0, pos + b0 + k);
+        tmp.resize(padded, pos[b0]);
+        PB_CUDA(m.load_positions(tmp.data(), padded, s));
+        PB_CUDA(m.forward_backward(padded, false, s));
+        PB_CUDA(cudaMemcpyAsync(out + (size_t)b0 * MLP_OUT, m.y, sizeof(float) * MLP_OUT * k, cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+    }
+    return PB_OK;
+}
+
+int pb_perft_batch_planned(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uint64_t *counts,
+                           pb_plan_stats *stats)
+{
+    if (!ctx || !roots || !depths || !counts || n < 0) return PB_ERR_ARG;
+    if (!ctx->gpu) return fail(ctx, PB_ERR_NODEVICE, "context has no GPU");
+    if (!ctx->mlp.ready) return fail(ctx, PB_ERR_ARG, "planner needs a trained network (pb_mlp_init/train)");
+    for (int i = 0; i < n; i++)
+        if (depths[i] < 0 || depths[i] > 12) return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    memset(&ctx->stats, 0, sizeof(ctx->stats));
+    if (stats) memset(stats, 0, sizeof(*stats));
+    int rc = plan_and_run(ctx, roots, depths, n, counts, stats);
+    for (int i = 0; i < n && rc == PB_OK; i++) ctx->stats.nodes += counts[i];
+    return rc;
 }
 
 }  // extern "C"

@@ -567,3 +567,270 @@ __global__ void __launch_bounds__(256) k_leaf1_rooted(const Board *__restrict__ 
 }
 
 }  // namespace pb
+
+namespace pb {
+
+// ---------------------------------------------------------------- graph-captured batch
+// Variants of the batched-level kernels whose sizes live in device memory, so
+// a whole batched perft (every level and the leaf) can be captured once as a
+// CUDA graph and replayed without host round trips.  Buffers have fixed
+// capacities planned on the host (from the learned size predictions); a level
+// that outgrows its capacity sets OVERFLOW in the error word, writes nothing
+// past the capacity, and the host then reruns the batch with exact sizing.
+enum : u32 { DEVERR_OVERFLOW = 4u };
+
+__device__ __forceinline__ u64 dev_size(const u64 *n_dev, u64 cap, u32 *err)
+{
+    u64 n = *n_dev;
+    if (n > cap) {
+        atomicOr(err, DEVERR_OVERFLOW);
+        n = cap;
+    }
+    return n;
+}
+
+// Scan with a device-resident length (grid = tiles of the capacity; surplus
+// CTAs take a ticket and leave).
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_dev(const u32 *__restrict__ in, const u64 *__restrict__ n_dev,
+                                                           u64 cap, u64 *__restrict__ out, u64 *__restrict__ status,
+                                                           u32 *__restrict__ ticket, u64 *__restrict__ total,
+                                                           u32 *__restrict__ err)
+{
+    __shared__ u32 s_tile;
+    const u64 n = dev_size(n_dev, cap, err);
+    const u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    if ((u64)s_tile >= tiles) {
+        if (n == 0 && s_tile == 0 && threadIdx.x == 0) *total = 0;
+        return;
+    }
+    __shared__ u64 s_warp[SCAN_THREADS / 32];
+    __shared__ u64 s_exclusive;
+    const u32 tile = s_tile;
+    const u64 base = (u64)tile * SCAN_TILE + (u64)threadIdx.x * SCAN_ITEMS;
+    u32 v[SCAN_ITEMS];
+    u64 local = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        v[k] = (base + k < n) ? in[base + k] : 0u;
+        local += v[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u64 x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        u64 y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        u64 w = (lane < SCAN_THREADS / 32) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < SCAN_THREADS / 32; o <<= 1) {
+            u64 y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < SCAN_THREADS / 32) s_warp[lane] = w;
+    }
+    __syncthreads();
+    const u64 block_total = s_warp[SCAN_THREADS / 32 - 1];
+    u64 thread_excl = x - local + (warp ? s_warp[warp - 1] : 0);
+    if (threadIdx.x == 0) {
+        u64 excl = 0;
+        if (tile == 0) {
+            st_release(status, ST_PREFIX | block_total);
+        } else {
+            st_release(status + tile, ST_AGG | block_total);
+            long long p = (long long)tile - 1;
+            u32 spins = 0;
+            while (p >= 0) {
+                u64 w = ld_acquire(status + p);
+                if ((w >> 62) == 0) {
+                    if (++spins > SCAN_SPIN_LIMIT) {
+                        atomicOr(err, DEVERR_SCAN_TIMEOUT);
+                        break;
+                    }
+                    continue;
+                }
+                excl += w & ST_VALUE;
+                if ((w >> 62) == 2) break;
+                p--;
+            }
+            st_release(status + tile, ST_PREFIX | (excl + block_total));
+        }
+        s_exclusive = excl;
+        if ((u64)(tile + 1) * SCAN_TILE >= n) *total = excl + block_total;
+    }
+    __syncthreads();
+    u64 run = s_exclusive + thread_excl;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+}
+
+// Generation with device-resident sizes: positions [0, npos) (npos from the
+// previous level), offsets and total from the scan; writes stay below `cap`.
+template <int C>
+__global__ void __launch_bounds__(GEN_THREADS) k_generate_dev(const Board *__restrict__ boards,
+                                                              const uint8_t *__restrict__ states,
+                                                              const u64 *__restrict__ offs,
+                                                              const u64 *__restrict__ total_dev,
+                                                              const u64 *__restrict__ npos_dev, u64 npos_cap, u64 cap,
+                                                              uint16_t *__restrict__ out_mv, u32 *__restrict__ out_pi,
+                                                              u32 *__restrict__ err)
+{
+    __shared__ uint16_t s_mv[GEN_CAP];
+    __shared__ u32 s_pi[GEN_CAP];
+    const u64 n = dev_size(npos_dev, npos_cap, err);
+    const u64 total = *total_dev;
+    const u64 first = (u64)blockIdx.x * GEN_THREADS;
+    if (first >= n) return;
+    const u64 last = min(first + GEN_THREADS, n);
+    const u64 tile_begin = offs[first];
+    const u64 tile_end = (last < n) ? offs[last] : total;
+    const u64 i = first + threadIdx.x;
+    const bool staged = (tile_end - tile_begin) <= (u64)GEN_CAP;
+    if (i < n) {
+        Board b = load_board(boards + i);
+        u32 st = states[i];
+        const u64 mine_begin = offs[i];
+        u64 mine_end = (i + 1 < n) ? offs[i + 1] : total;
+        bool over = false;
+        if (mine_end > cap) {
+            atomicOr(err, DEVERR_OVERFLOW);
+            mine_end = cap;
+        }
+        if (mine_end <= mine_begin) {
+        } else if (staged) {
+            SmemSink s{s_mv, s_pi, (u32)i, (int)(mine_begin - tile_begin), (int)(mine_end - tile_begin), false};
+            gen_moves<C>(b, st, s);
+            over = s.over || s.n < s.cap;
+        } else {
+            GlobalSink s{out_mv, out_pi, (u32)i, mine_begin, mine_end, false};
+            gen_moves<C>(b, st, s);
+            over = s.over || s.n < s.cap;
+        }
+        if (over && total <= cap) atomicOr(err, DEVERR_CAPACITY);
+    }
+    if (!staged) return;
+    __syncthreads();
+    const u64 end = min(tile_end, cap);
+    const int cnt = end > tile_begin ? (int)(end - tile_begin) : 0;
+    for (int k = threadIdx.x; k < cnt; k += GEN_THREADS) {
+        out_mv[tile_begin + k] = s_mv[k];
+        out_pi[tile_begin + k] = s_pi[k];
+    }
+}
+
+template <int C>
+__global__ void __launch_bounds__(256) k_expand_rooted_dev(const Board *__restrict__ pboards,
+                                                           const uint8_t *__restrict__ pstates,
+                                                           const u32 *__restrict__ proot,
+                                                           const u32 *__restrict__ pidx,
+                                                           const uint16_t *__restrict__ moves,
+                                                           const u64 *__restrict__ n_dev, u64 cap,
+                                                           const u64 *__restrict__ npar_dev, u64 npar_cap,
+                                                           Board *__restrict__ cboards, uint8_t *__restrict__ cstates,
+                                                           u32 *__restrict__ croot, u32 *__restrict__ counts,
+                                                           u32 *__restrict__ err)
+{
+    const u64 n = dev_size(n_dev, cap, err);
+    const u64 npar = min(*npar_dev, npar_cap);
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        u32 p = pidx[i];
+        if (p >= npar) {
+            counts[i] = 0;
+            croot[i] = 0;
+            atomicOr(err, DEVERR_CAPACITY);
+            continue;
+        }
+        Board b = load_board(pboards + p);
+        u32 st = pstates[p];
+        make_move<C>(b, st, moves[i]);
+        store_board(cboards + i, b);
+        cstates[i] = (uint8_t)st;
+        croot[i] = proot[p];
+        counts[i] = count_moves<1 - C, true>(b, st);
+    }
+}
+
+// Persistent two-ply leaf driven by a device work queue: each warp takes
+// 32-edge chunks from an atomic cursor until the level is exhausted, so
+// uneven subtrees balance across the SMs without a per-edge grid.
+template <int C, bool STRICT>
+__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
+    k_leaf2_rooted_queue(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                         const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
+                         const uint16_t *__restrict__ moves, const u64 *__restrict__ n_dev, u64 cap,
+                         const u64 *__restrict__ npar_dev, u64 npar_cap, unsigned long long *__restrict__ cursor,
+                         unsigned long long *__restrict__ root_counts, unsigned long long *__restrict__ counter,
+                         u32 *__restrict__ err)
+{
+    const u64 n = dev_size(n_dev, cap, err);
+    const u64 npar = min(*npar_dev, npar_cap);
+    const int lane = threadIdx.x & 31;
+    u32 counted = 0;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(cursor, 32ULL);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const u64 i = base + lane;
+        u32 total = 0, root = 0;
+        bool valid = i < n && pidx[i] < npar;
+        if (valid) {
+            u32 p = pidx[i];
+            root = proot[p];
+            Board b = load_board(pboards + p);
+            u32 st = pstates[p];
+            make_move<C>(b, st, moves[i]);
+            uint16_t mv[MAX_MOVES];
+            ArraySink sink{mv, 0};
+            gen_moves<1 - C>(b, st, sink);
+            for (int k = 0; k < sink.n; k++) {
+                Board g = b;
+                u32 gs = st;
+                make_move<1 - C>(g, gs, mv[k]);
+                total += count_moves<C, STRICT>(g, gs);
+            }
+            counted += sink.n;
+        }
+        add_by_key(root_counts, root, total, valid);
+    }
+    counted = __reduce_add_sync(0xffffffffu, counted);
+    if (lane == 0 && counted) atomicAdd(counter + 1, (unsigned long long)counted);
+}
+
+template <int C, bool STRICT>
+__global__ void __launch_bounds__(256) k_leaf1_rooted_dev(const Board *__restrict__ pboards,
+                                                          const uint8_t *__restrict__ pstates,
+                                                          const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
+                                                          const uint16_t *__restrict__ moves,
+                                                          const u64 *__restrict__ n_dev, u64 cap,
+                                                          const u64 *__restrict__ npar_dev, u64 npar_cap,
+                                                          unsigned long long *__restrict__ root_counts,
+                                                          u32 *__restrict__ err)
+{
+    const u64 n = dev_size(n_dev, cap, err);
+    const u64 npar = min(*npar_dev, npar_cap);
+    for (u64 base = (u64)blockIdx.x * blockDim.x; base < n; base += (u64)gridDim.x * blockDim.x) {
+        u64 i = base + threadIdx.x;
+        u32 cnt = 0, root = 0;
+        bool valid = i < n && pidx[i] < npar;
+        if (valid) {
+            u32 p = pidx[i];
+            root = proot[p];
+            Board b = load_board(pboards + p);
+            u32 st = pstates[p];
+            make_move<C>(b, st, moves[i]);
+            cnt = count_moves<1 - C, STRICT>(b, st);
+        }
+        add_by_key(root_counts, root, cnt, valid);
+    }
+}
+
+}  // namespace pb

@@ -1,0 +1,56 @@
+"""Learned batch planner: predicted level sizes, bin-packing, root splitting
+and graph-captured batches must give exactly the counts of the plain batched
+path - also when the plan is wrong (overflow -> exact rerun)."""
+import numpy as np
+import pytest
+
+import perft_gpu_2026_b200 as pg
+
+pytestmark = pytest.mark.gpu
+
+
+def _train(eng, n=3072, seed=90_000):
+    pos = [pg.random_playout(seed + i, i % 60)[0] for i in range(n)]
+    pos = [p for p in pos if pg.count_moves(p, True) > 0]
+    counts = np.array([eng.perft_batch(pos, [d] * len(pos)) for d in (1, 2, 3, 4)], dtype=np.float64).T
+    t = np.log2(1.0 + counts)
+    eng.mlp_init(seed=5, out_bias=list(t.mean(0)))
+    eng.mlp_train(pos, t, epochs=20, batch=256, lr=2e-3)
+
+
+def test_planned_batch_matches_exact_counts():
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=4 << 30)
+    _train(eng)
+    roots = pg.uneven_roots(200, 6, 40, seed=31)
+    depths = [2 + (i % 4) for i in range(len(roots))]
+    got, st = eng.perft_batch_planned(roots, depths)
+    assert got == eng.perft_batch(roots, depths)
+    assert st.graph_batches >= 1
+    eng.close()
+
+
+def test_wrong_plan_reruns_exactly():
+    # an untrained network predicting ~0 for every level: every batch
+    # overflows its plan and is rerun with exact sizing
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
+    eng.mlp_init(seed=9, out_bias=[0.0, 0.0, 0.0, 0.0])
+    params = eng.mlp_params()
+    params[:] = 0.0
+    eng.mlp_set_params(params)
+    roots = pg.uneven_roots(64, 6, 40, seed=32)
+    got, st = eng.perft_batch_planned(roots, [5] * len(roots))
+    assert got == eng.perft_batch(roots, [5] * len(roots))
+    assert st.retries >= 1
+    eng.close()
+
+
+def test_large_roots_are_split():
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=64 << 20)
+    _train(eng, n=1024, seed=91_000)
+    roots = [pg.config_position(4, 1), pg.parse_fen(pg.START_FEN)]
+    got, st = eng.perft_batch_planned(roots, [6, 6])
+    ref = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30)
+    assert got == [ref.perft_position(r, 6) for r in roots]
+    assert st.split_roots >= 1
+    ref.close()
+    eng.close()
