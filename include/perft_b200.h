@@ -167,6 +167,12 @@ int pb_get_tuning(const pb_ctx *ctx, pb_tuning *t);
 int pb_set_timing(pb_ctx *ctx, int enable);
 int pb_last_stats(const pb_ctx *ctx, pb_stats *out);
 
+/* n playouts at once (threads): position i uses the generator state drawn
+ * i-th from a splitmix64 stream seeded with `seed`; from that state it draws
+ * its length uniformly in [min_plies, max_plies], then plays as
+ * pb_random_playout.  played[i] (optional) = plies actually played. */
+int pb_random_playouts(uint64_t seed, int n, int min_plies, int max_plies, pb_pos *out, int *played);
+
 /* Device kernels on caller-owned device buffers, for tests: exclusive scan of
  * n u32 counts into n u64 offsets and a device u64 total. */
 int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total);

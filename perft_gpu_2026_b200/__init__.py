@@ -122,6 +122,8 @@ def _load() -> ctypes.CDLL:
         "pb_generate_moves": (ctypes.c_int, [P(Pos), P(ctypes.c_uint16)]),
         "pb_make_move": (ctypes.c_int, [P(Pos), ctypes.c_uint16]),
         "pb_random_playout": (ctypes.c_int, [P(ctypes.c_uint64), ctypes.c_int, P(Pos)]),
+        "pb_random_playouts": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(Pos),
+                                               P(ctypes.c_int)]),
         "pb_device_count": (ctypes.c_int, []),
         "pb_choose_launch_depth": (ctypes.c_int, [ctypes.c_void_p, P(Pos)]),
         "pb_prepare": (ctypes.c_int, [ctypes.c_void_p, P(Pos), ctypes.c_int]),
@@ -218,6 +220,16 @@ def random_playout(seed_state: int, plies: int) -> Tuple[Pos, int, int]:
     p = Pos()
     n = lib.pb_random_playout(ctypes.byref(st), plies, ctypes.byref(p))
     return p, n, st.value
+
+
+def random_playouts(seed: int, n: int, min_plies: int, max_plies: int) -> List[Pos]:
+    """n playouts (threaded in the library); position i's generator state is
+    the i-th splitmix64 draw of `seed`, its length uniform in [min, max]."""
+    arr = (Pos * n)()
+    rc = lib.pb_random_playouts(seed, n, min_plies, max_plies, arr, None)
+    if rc != PB_OK:
+        raise PerftError(rc, "pb_random_playouts failed")
+    return list(arr)
 
 
 def splitmix64(state: int) -> Tuple[int, int]:

@@ -19,6 +19,7 @@
 #include <chrono>
 #include <string>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/perft_b200.h"
@@ -1148,6 +1149,40 @@ int plan_and_run(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uin
     return PB_OK;
 }
 
+// ---------------------------------------------------------------- workload generator
+// Sort key equal to the order of the moves' UCI text: from file, from rank,
+// to file, to rank, then the promotion letter ("" < b < n < q < r).
+inline u32 uci_key(uint16_t m)
+{
+    static const u32 promo_rank[4] = {2, 1, 4, 3};  // flags&3: N, B, R, Q -> n=2, b=1, r=4, q=3
+    int from = move_from(m), to = move_to(m), fl = move_flags(m);
+    u32 k = (u32)(((from & 7) * 8 + (from >> 3)) * 64 + (to & 7) * 8 + (to >> 3));
+    return k * 5 + ((fl & MF_PROMO) ? promo_rank[fl & 3] : 0);
+}
+
+// `plies` uniformly random legal moves from the initial array (fewer at a
+// terminal position); returns the plies played.
+int playout(u64 *st, int plies, pb_pos *out)
+{
+    parse_fen("rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1", out);
+    Board b = to_board(*out);
+    u32 s = out->state;
+    int c = WHITE, played = 0;
+    for (int i = 0; i < plies; i++) {
+        uint16_t mv[MAX_MOVES];
+        int n = host_gen(b, s, c, mv);
+        if (n <= 0) break;
+        std::sort(mv, mv + n, [](uint16_t a, uint16_t z) { return uci_key(a) < uci_key(z); });
+        u64 r = splitmix64(st);
+        u32 pick = (u32)(((unsigned __int128)r * (u32)n) >> 64);
+        host_make(b, s, c, mv[pick]);
+        c = 1 - c;
+        played++;
+    }
+    to_pos(b, s, c, *out);
+    return played;
+}
+
 // ---------------------------------------------------------------- 128-bit helpers
 inline void add128(pb_u128 &a, const pb_u128 &b)
 {
@@ -1505,22 +1540,31 @@ int pb_random_playout(uint64_t *rng_state, int plies, pb_pos *out)
 {
     if (!rng_state || !out || plies < 0) return PB_ERR_ARG;
     build_host_tables();
-    parse_fen("rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1", out);
-    int played = 0;
-    for (int i = 0; i < plies; i++) {
-        uint16_t mv[MAX_MOVES];
-        int n = pb_generate_moves(out, mv);
-        if (n <= 0) break;
-        std::vector<std::pair<std::string, uint16_t>> keyed;
-        keyed.reserve(n);
-        for (int k = 0; k < n; k++) keyed.emplace_back(move_uci(mv[k]), mv[k]);
-        std::sort(keyed.begin(), keyed.end());
-        u64 r = splitmix64(reinterpret_cast<u64 *>(rng_state));
-        u32 pick = (u32)(((unsigned __int128)r * (u32)n) >> 64);
-        pb_make_move(out, keyed[pick].second);
-        played++;
-    }
-    return played;
+    return playout(reinterpret_cast<u64 *>(rng_state), plies, out);
+}
+
+int pb_random_playouts(uint64_t seed, int n, int min_plies, int max_plies, pb_pos *out, int *played)
+{
+    if (!out || n < 0 || min_plies < 0 || max_plies < min_plies) return PB_ERR_ARG;
+    build_host_tables();
+    // per-position generator states: the i-th draw of the master stream
+    std::vector<u64> seeds(n);
+    u64 master = seed;
+    for (int i = 0; i < n; i++) seeds[i] = splitmix64(&master);
+    const u64 span = (u64)(max_plies - min_plies + 1);
+    unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; t++)
+        pool.emplace_back([&, t]() {
+            for (int i = (int)t; i < n; i += (int)nt) {
+                u64 st = seeds[i];
+                int plies = min_plies + (int)(((unsigned __int128)splitmix64(&st) * span) >> 64);
+                int k = playout(&st, plies, &out[i]);
+                if (played) played[i] = k;
+            }
+        });
+    for (auto &th : pool) th.join();
+    return PB_OK;
 }
 
 int pb_perft_batch(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uint64_t *counts)

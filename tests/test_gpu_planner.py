@@ -48,9 +48,9 @@ def test_large_roots_are_split():
     eng = pg.Engine(device=0, use_tt=False, arena_bytes=64 << 20)
     _train(eng, n=1024, seed=91_000)
     roots = [pg.config_position(4, 1), pg.parse_fen(pg.START_FEN)]
-    got, st = eng.perft_batch_planned(roots, [6, 6])
+    got, st = eng.perft_batch_planned(roots, [7, 7])
     ref = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 30)
-    assert got == [ref.perft_position(r, 6) for r in roots]
+    assert got == [ref.perft_position(r, 7) for r in roots]
     assert st.split_roots >= 1
     ref.close()
     eng.close()
