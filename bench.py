@@ -198,6 +198,7 @@ def main():
     ap.add_argument("--depth", type=int, default=WORKLOAD["depth"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--leaf-kernel", type=int, default=0, help="1 = edge per thread, 2 = cooperative (0 = engine default)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default launch parameters")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -222,9 +223,14 @@ def main():
     root = pg.config_position(4, 1)
     depth = args.depth
     eng = pg.Engine(device=local, use_tt=False)
-    eng.set_timing(True)
+    tuning = None
     if args.leaf_kernel:
         eng.set_tuning(leaf_kernel=args.leaf_kernel)
+    elif not args.no_autotune:
+        from perft_gpu_2026_b200 import autotune
+
+        tuning = autotune.load_or_tune(eng, local)["best"]
+    eng.set_timing(True)
 
     # shard: depth-2 subtrees round-robin over ranks (one rank: the whole root)
     from perft_gpu_2026_b200 import dist as pdist
@@ -311,7 +317,8 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": my_ms, "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
                 "config": dict(WORKLOAD, depth=depth, nodes=nodes, l2="flushed (256 MB write) before each step",
-                               parallelism=f"depth-2 subtrees over {world} rank(s)"),
+                               parallelism=f"depth-2 subtrees over {world} rank(s)",
+                               tuning=eng.get_tuning().as_dict()),
                 "e2e": {"value": nodes / (my_e2e / 1e3), "unit": METRIC, "ms_per_step": my_e2e,
                         "h2d_bytes_per_step": int(results[0][5]), "d2h_bytes_per_step": int(results[0][6]),
                         "timing": "host wall clock around pb_perft_position"},

@@ -157,7 +157,10 @@ typedef struct {
 typedef struct {
     int leaf_kernel;
     int leaf_blocks_per_sm;
-    int reserved[6];
+    int leaf_threads;   /* CTA size of the one-edge-per-thread leaf: 128, 256 (default) or 512 */
+    int gen_threads;    /* CTA size of the staged generator: 64 or 128 (default); stages 64 moves per thread */
+    int leaf_fuse;      /* plies fused in the leaf kernel: 2 (default) or 1 (one more BFS level) */
+    int reserved[3];
 } pb_tuning;
 
 int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t);

@@ -86,7 +86,12 @@ class Tuning(ctypes.Structure):
     """pb_tuning: launch parameters (zero = keep current)."""
 
     _fields_ = [("leaf_kernel", ctypes.c_int), ("leaf_blocks_per_sm", ctypes.c_int),
-                ("reserved", ctypes.c_int * 6)]
+                ("leaf_threads", ctypes.c_int), ("gen_threads", ctypes.c_int), ("leaf_fuse", ctypes.c_int),
+                ("reserved", ctypes.c_int * 3)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k in ("leaf_kernel", "leaf_blocks_per_sm", "leaf_threads", "gen_threads",
+                                              "leaf_fuse")}
 
 
 class PlanStats(ctypes.Structure):
@@ -364,10 +369,14 @@ class Engine:
     def set_timing(self, enable: bool = True) -> None:
         self._check(lib.pb_set_timing(self._h, int(enable)))
 
-    def set_tuning(self, leaf_kernel: int = 0, leaf_blocks_per_sm: int = 0) -> None:
+    def set_tuning(self, leaf_kernel: int = 0, leaf_blocks_per_sm: int = 0, leaf_threads: int = 0,
+                   gen_threads: int = 0, leaf_fuse: int = 0) -> None:
         t = Tuning()
         t.leaf_kernel = leaf_kernel
         t.leaf_blocks_per_sm = leaf_blocks_per_sm
+        t.leaf_threads = leaf_threads
+        t.gen_threads = gen_threads
+        t.leaf_fuse = leaf_fuse
         self._check(lib.pb_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self) -> Tuning:

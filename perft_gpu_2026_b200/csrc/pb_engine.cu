@@ -70,7 +70,7 @@ struct pb_ctx {
     u64 *h_pinned = nullptr;  // pinned host words for readbacks
     int launch_depth = 0;
     bool timing = false;
-    pb_tuning tuning{1, 0, {0, 0, 0, 0, 0, 0}};
+    pb_tuning tuning{1, 0, 256, 128, 2, {0, 0, 0}};
     int num_sms = 0;
     uint16_t *spill = nullptr;  // cooperative-leaf spill area (device)
     size_t spill_blocks = 0;
@@ -181,8 +181,17 @@ template <int C, bool S>
 int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi, const uint16_t *mv, u64 n, u64 npar)
 {
     cudaStream_t s = ctx->stream;
+    if (ctx->tuning.leaf_fuse == 1) {
+        k_leaf1<C, S><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter);
+        PB_CUDA(cudaGetLastError());
+        return PB_OK;
+    }
     if (ctx->tuning.leaf_kernel == 1) {
-        k_leaf2<C, S><<<grid_for(n, PB_LEAF_THREADS), PB_LEAF_THREADS, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter);
+        switch (ctx->tuning.leaf_threads) {
+        case 128: k_leaf2<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        case 512: k_leaf2<C, S, 512><<<grid_for(n, 512), 512, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        default: k_leaf2<C, S, 256><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        }
         PB_CUDA(cudaGetLastError());
         return PB_OK;
     }
@@ -206,6 +215,20 @@ int launch_leaf(pb_ctx *ctx, int c, bool strict, const Board *b, const uint8_t *
                                   : launch_leaf_t<WHITE, false>(ctx, b, st, pi, mv, n, npar);
     return strict ? launch_leaf_t<BLACK, true>(ctx, b, st, pi, mv, n, npar)
                   : launch_leaf_t<BLACK, false>(ctx, b, st, pi, mv, n, npar);
+}
+
+// Staged generation with the tuned CTA size.
+void launch_generate(pb_ctx *ctx, int c, const Board *b, const uint8_t *st, const u64 *offs, u64 n, uint16_t *mv,
+                     u32 *pi)
+{
+    cudaStream_t s = ctx->stream;
+    if (ctx->tuning.gen_threads == 64) {
+        if (c == WHITE) k_generate<WHITE, 64><<<grid_for(n, 64), 64, 0, s>>>(b, st, offs, ctx->d_total, n, mv, pi, ctx->d_err);
+        else k_generate<BLACK, 64><<<grid_for(n, 64), 64, 0, s>>>(b, st, offs, ctx->d_total, n, mv, pi, ctx->d_err);
+    } else {
+        if (c == WHITE) k_generate<WHITE, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, offs, ctx->d_total, n, mv, pi, ctx->d_err);
+        else k_generate<BLACK, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, offs, ctx->d_total, n, mv, pi, ctx->d_err);
+    }
 }
 
 // One GPU breadth-first perft; status BFS_TOO_BIG when a level would not fit.
@@ -249,7 +272,8 @@ int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth,
     u64 n = (u64)n0;
     u64 n_par = 1;  // positions the current edges point into
     int c = color;
-    for (int rem = depth - 1; rem > 2; rem--) {
+    const int fuse = ctx->tuning.leaf_fuse == 1 ? 1 : 2;
+    for (int rem = depth - 1; rem > fuse; rem--) {
         Board *cb = ar.take<Board>(n);
         uint8_t *cs = ar.take<uint8_t>(n);
         u32 *cnt = ar.take<u32>(n);
@@ -292,10 +316,7 @@ int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth,
             *bfs_status = BFS_TOO_BIG;
             return PB_OK;
         }
-        if (c == WHITE)
-            k_generate<BLACK><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n, nmv, npi, ctx->d_err);
-        else
-            k_generate<WHITE><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(cb, cs, offs, ctx->d_total, n, nmv, npi, ctx->d_err);
+        launch_generate(ctx, 1 - c, cb, cs, offs, n, nmv, npi);
         PB_CUDA(cudaGetLastError());
         stats.kernels += 1;
         cur_b = cb;
@@ -1439,6 +1460,18 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
     if (t->leaf_blocks_per_sm) {
         if (t->leaf_blocks_per_sm < 0 || t->leaf_blocks_per_sm > 8) return PB_ERR_ARG;
         ctx->tuning.leaf_blocks_per_sm = t->leaf_blocks_per_sm;
+    }
+    if (t->leaf_threads) {
+        if (t->leaf_threads != 128 && t->leaf_threads != 256 && t->leaf_threads != 512) return PB_ERR_ARG;
+        ctx->tuning.leaf_threads = t->leaf_threads;
+    }
+    if (t->gen_threads) {
+        if (t->gen_threads != 64 && t->gen_threads != 128) return PB_ERR_ARG;
+        ctx->tuning.gen_threads = t->gen_threads;
+    }
+    if (t->leaf_fuse) {
+        if (t->leaf_fuse != 1 && t->leaf_fuse != 2) return PB_ERR_ARG;
+        ctx->tuning.leaf_fuse = t->leaf_fuse;
     }
     return PB_OK;
 }

@@ -213,21 +213,22 @@ struct GlobalSink {
     }
 };
 
-template <int C>
-__global__ void __launch_bounds__(GEN_THREADS) k_generate(const Board *__restrict__ boards,
-                                                          const uint8_t *__restrict__ states,
-                                                          const u64 *__restrict__ offs, const u64 *__restrict__ total,
-                                                          u64 n, uint16_t *__restrict__ out_mv,
-                                                          u32 *__restrict__ out_pi, u32 *__restrict__ err)
+template <int C, int GT = GEN_THREADS>
+__global__ void __launch_bounds__(GT) k_generate(const Board *__restrict__ boards,
+                                                 const uint8_t *__restrict__ states,
+                                                 const u64 *__restrict__ offs, const u64 *__restrict__ total,
+                                                 u64 n, uint16_t *__restrict__ out_mv,
+                                                 u32 *__restrict__ out_pi, u32 *__restrict__ err)
 {
-    __shared__ uint16_t s_mv[GEN_CAP];
-    __shared__ u32 s_pi[GEN_CAP];
-    const u64 first = (u64)blockIdx.x * GEN_THREADS;
-    const u64 last = min(first + GEN_THREADS, n);  // exclusive
+    constexpr int CAP = GT * 64;  // staged moves per CTA (6 B each)
+    __shared__ uint16_t s_mv[CAP];
+    __shared__ u32 s_pi[CAP];
+    const u64 first = (u64)blockIdx.x * GT;
+    const u64 last = min(first + GT, n);  // exclusive
     const u64 tile_begin = offs[first];
     const u64 tile_end = (last < n) ? offs[last] : *total;
     const u64 i = first + threadIdx.x;
-    const bool staged = (tile_end - tile_begin) <= (u64)GEN_CAP;
+    const bool staged = (tile_end - tile_begin) <= (u64)CAP;
     if (i < n) {
         Board b = load_board(boards + i);
         u32 st = states[i];
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(GEN_THREADS) k_generate(const Board *__restric
     if (!staged) return;
     __syncthreads();
     const int cnt = (int)(tile_end - tile_begin);
-    for (int k = threadIdx.x; k < cnt; k += GEN_THREADS) {
+    for (int k = threadIdx.x; k < cnt; k += GT) {
         out_mv[tile_begin + k] = s_mv[k];
         out_pi[tile_begin + k] = s_pi[k];
     }
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(GEN_THREADS) k_generate(const Board *__restric
 
 // ---------------------------------------------------------------- leaves
 // One-ply leaf: the move count of each edge's child (perft 1 of the child).
-template <int C>
+template <int C, bool STRICT>
 __global__ void __launch_bounds__(256) k_leaf1(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                                                const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves, u64 n,
                                                u64 nparents, unsigned long long *__restrict__ counter)
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(256) k_leaf1(const Board *__restrict__ pboards
         Board b = load_board(pboards + p);
         u32 st = pstates[p];
         make_move<C>(b, st, moves[i]);
-        cnt = count_moves<1 - C, false>(b, st);
+        cnt = count_moves<1 - C, STRICT>(b, st);
     }
     cnt = __reduce_add_sync(0xffffffffu, cnt);
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(counter, (unsigned long long)cnt);
@@ -287,8 +288,8 @@ __global__ void __launch_bounds__(256) k_leaf1(const Board *__restrict__ pboards
 #ifndef PB_LEAF_MIN_BLOCKS
 #define PB_LEAF_MIN_BLOCKS 4
 #endif
-template <int C, bool STRICT>
-__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS) k_leaf2(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+template <int C, bool STRICT, int T = PB_LEAF_THREADS>
+__global__ void __launch_bounds__(T, 1024 / T) k_leaf2(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                                                const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves, u64 n,
                                                u64 nparents, unsigned long long *__restrict__ counter)
 {

@@ -172,3 +172,25 @@ def test_batch_splits_when_arena_is_small():
     assert got == [ref.perft_position(r, 5) for r in roots]
     eng.close()
     ref.close()
+
+
+@pytest.mark.parametrize("cfg", [dict(leaf_threads=128), dict(leaf_threads=512), dict(gen_threads=64),
+                                 dict(leaf_fuse=1)])
+def test_tuned_launch_parameters_keep_counts(cfg, golden):
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
+    eng.set_tuning(**cfg)
+    for case in golden[:30]:
+        p = pg.parse_fen(case["fen"])
+        for d, want in enumerate(case["counts"], start=1):
+            assert eng.perft_position(p, d) == want, (cfg, case["name"], d)
+    eng.close()
+
+
+def test_autotune_picks_a_candidate():
+    from perft_gpu_2026_b200 import autotune
+
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
+    res = autotune.tune(eng, depth=5)
+    assert res["best"] in autotune.candidates()
+    assert eng.get_tuning().as_dict()["leaf_threads"] == res["best"]["leaf_threads"]
+    eng.close()
