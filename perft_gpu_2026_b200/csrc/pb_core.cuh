@@ -54,12 +54,15 @@ constexpr u64 FILEH = 0x8080808080808080ULL;
 constexpr u64 PROMO_RANKS = RANK1 | RANK8;
 
 // Slider magic entry: attacks = table[offset + ((occ & mask) * magic) >> (64 - bits)].
+// `base` is the slice's offset into the attack table on the host and, in the
+// device copy, the slice's device address, so a lookup ends in one IMAD-based
+// address computation and one load.
 struct __align__(32) Magic {
     u64 mask;
     u64 magic;
-    u32 offset;
-    u32 shift;  // 64 - bits
-    u64 pad;
+    u64 base;
+    u32 shift_hi;  // 32 - bits: the index is the product's high word >> shift_hi
+    u32 shift;     // 64 - bits
 };
 
 // Attack and geometry tables.  One copy lives in device global memory
@@ -140,14 +143,14 @@ PB_HD u64 magic_lookup(const Magic *e, u64 occ)
 {
 #ifdef __CUDA_ARCH__
     // bits <= 12, so the index lies in the high word of the product: one
-    // 32-bit shift by (shift - 32) instead of a 64-bit variable shift
+    // 32-bit shift instead of a 64-bit variable shift
     ulonglong2 mm = __ldg(reinterpret_cast<const ulonglong2 *>(e));
-    uint2 os = __ldg(reinterpret_cast<const uint2 *>(&e->offset));
+    ulonglong2 bs = __ldg(reinterpret_cast<const ulonglong2 *>(&e->base));
     u32 hi = (u32)(((occ & mm.x) * mm.y) >> 32);
-    return __ldg(&g_attacks[os.x + (hi >> (os.y - 32))]);
+    return __ldg(reinterpret_cast<const u64 *>(bs.x) + (hi >> (u32)bs.y));
 #else
     u64 idx = ((occ & e->mask) * e->magic) >> e->shift;
-    return h_attacks[e->offset + (u32)idx];
+    return h_attacks[e->base + (u32)idx];
 #endif
 }
 PB_HD u64 rook_att(int sq, u64 occ) { return magic_lookup(&PB_TAB.rook[sq], occ); }
@@ -297,18 +300,12 @@ PB_HD u32 count_evasions(const Sets &s, u32 state, u64 pinned, u64 threat, int k
     return n;
 }
 
-// Number of legal moves (countMoves, MoveGeneratorBitboard.h:1700-1943).
+// Legal-move count when the side to move is not in check (the main part of
+// countMoves, MoveGeneratorBitboard.h:1729-1943).
 template <int C, bool STRICT>
-PB_HD u32 count_moves(const Board &b, u32 state)
+PB_HD u32 count_quiet(const Sets &s, u32 state, u64 pinned, u64 threat, int ksq)
 {
-    Sets s = derive<C>(b);
-    u64 my_king = s.kings & s.us;
-    int ksq = bit_index(my_king);
-    u64 eb = s.bq & s.them, er = s.rq & s.them;
-    u64 pinned = pinned_set(ksq, eb, er, s.occ);
-    u64 threat = enemy_attacks<C>(s, my_king);
-    if (threat & my_king) return count_evasions<C, STRICT>(s, state, pinned, threat, ksq);
-
+    const u64 er = s.rq & s.them;
     u32 n = 0;
     u64 empty = ~s.occ;
     u64 my_pawns = s.pawns & s.us;
@@ -394,6 +391,34 @@ PB_HD u32 count_moves(const Board &b, u32 state)
         }
     }
     return n;
+}
+
+// What every move count needs first: piece sets, king square, pinned pieces
+// and the enemy attack map (findPinnedPieces + findAttackedSquares).
+struct CountPrep {
+    Sets s;
+    u64 pinned, threat;
+    int ksq;
+};
+template <int C> PB_HD CountPrep count_prep(const Board &b)
+{
+    CountPrep p;
+    p.s = derive<C>(b);
+    u64 my_king = p.s.kings & p.s.us;
+    p.ksq = bit_index(my_king);
+    p.pinned = pinned_set(p.ksq, p.s.bq & p.s.them, p.s.rq & p.s.them, p.s.occ);
+    p.threat = enemy_attacks<C>(p.s, my_king);
+    return p;
+}
+template <int C> PB_HD bool prep_in_check(const CountPrep &p) { return (p.threat >> p.ksq) & 1; }
+
+// Number of legal moves (countMoves, MoveGeneratorBitboard.h:1700-1943).
+template <int C, bool STRICT>
+PB_HD u32 count_moves(const Board &b, u32 state)
+{
+    CountPrep p = count_prep<C>(b);
+    if (prep_in_check<C>(p)) return count_evasions<C, STRICT>(p.s, state, p.pinned, p.threat, p.ksq);
+    return count_quiet<C, STRICT>(p.s, state, p.pinned, p.threat, p.ksq);
 }
 
 // ---------------------------------------------------------------- generation

@@ -186,6 +186,14 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
         PB_CUDA(cudaGetLastError());
         return PB_OK;
     }
+    if (ctx->tuning.leaf_kernel == 3) {
+        switch (ctx->tuning.leaf_threads) {
+        case 128: k_leaf2_defer<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        default: k_leaf2_defer<C, S, 256><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        }
+        PB_CUDA(cudaGetLastError());
+        return PB_OK;
+    }
     if (ctx->tuning.leaf_kernel == 1) {
         switch (ctx->tuning.leaf_threads) {
         case 128: k_leaf2<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
@@ -1321,8 +1329,13 @@ int pb_create(int device, const pb_opts *opts, pb_ctx **out)
         int rc = PB_OK;
         do {
             if ((e = cudaSetDevice(device)) != cudaSuccess) { rc = cuda_fail(ctx, e, "cudaSetDevice"); break; }
-            if ((e = cudaMemcpyToSymbol(g_tab, &h_tab, sizeof(Tables))) != cudaSuccess) { rc = cuda_fail(ctx, e, "upload tables"); break; }
             if ((e = cudaMemcpyToSymbol(g_attacks, h_attacks, sizeof(h_attacks))) != cudaSuccess) { rc = cuda_fail(ctx, e, "upload attacks"); break; }
+            void *dev_att = nullptr;
+            if ((e = cudaGetSymbolAddress(&dev_att, g_attacks)) != cudaSuccess) { rc = cuda_fail(ctx, e, "attack table address"); break; }
+            {
+                Tables dt = device_tables(reinterpret_cast<const u64 *>(dev_att));
+                if ((e = cudaMemcpyToSymbol(g_tab, &dt, sizeof(Tables))) != cudaSuccess) { rc = cuda_fail(ctx, e, "upload tables"); break; }
+            }
             if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) { rc = cuda_fail(ctx, e, "stream"); break; }
             char *small = nullptr;
             if ((e = cudaMalloc(&small, 256)) != cudaSuccess) { rc = cuda_fail(ctx, e, "scratch"); break; }
@@ -1454,7 +1467,7 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
 {
     if (!ctx || !t) return PB_ERR_ARG;
     if (t->leaf_kernel) {
-        if (t->leaf_kernel < 1 || t->leaf_kernel > 2) return PB_ERR_ARG;
+        if (t->leaf_kernel < 1 || t->leaf_kernel > 3) return PB_ERR_ARG;
         ctx->tuning.leaf_kernel = t->leaf_kernel;
     }
     if (t->leaf_blocks_per_sm) {

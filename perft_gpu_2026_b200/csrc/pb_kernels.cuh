@@ -835,3 +835,96 @@ __global__ void __launch_bounds__(256) k_leaf1_rooted_dev(const Board *__restric
 }
 
 }  // namespace pb
+
+namespace pb {
+
+// ---------------------------------------------------------------- leaf with deferred evasions
+// The fused two-ply leaf, but a grandchild in check is not counted on the
+// spot: its board, state, pinned set and attack map go to a per-warp queue in
+// shared memory, and once 32 are queued the whole warp counts them together.
+// In-check positions are rare (about 1-2 % of the counted positions) but
+// frequent per warp (one lane in 32 often enough), and counting an evasion
+// costs about as much as counting a quiet position, so a warp that met one
+// used to pay for both paths on every such step.
+constexpr int DEFER_CAP = 64;  // <= 31 waiting + 32 new
+
+template <int C, bool STRICT, int T>
+__global__ void __launch_bounds__(T, 1024 / T) k_leaf2_defer(const Board *__restrict__ pboards,
+                                                             const uint8_t *__restrict__ pstates,
+                                                             const u32 *__restrict__ pidx,
+                                                             const uint16_t *__restrict__ moves, u64 n, u64 nparents,
+                                                             unsigned long long *__restrict__ counter)
+{
+    __shared__ Board q_b[T / 32][DEFER_CAP];
+    __shared__ u64 q_pin[T / 32][DEFER_CAP];
+    __shared__ u64 q_thr[T / 32][DEFER_CAP];
+    __shared__ uint8_t q_st[T / 32][DEFER_CAP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const u64 i = (u64)blockIdx.x * T + threadIdx.x;
+    u32 total = 0;
+    int nm = 0;
+    Board b;
+    u32 st = 0;
+    uint16_t mv[MAX_MOVES];
+    if (i < n && pidx[i] < nparents) {
+        u32 p = pidx[i];
+        b = load_board(pboards + p);
+        st = pstates[p];
+        make_move<C>(b, st, moves[i]);
+        ArraySink sink{mv, 0};
+        gen_moves<1 - C>(b, st, sink);
+        nm = sink.n;
+    }
+    const u32 counted = (u32)nm;
+    const int kmax = (int)__reduce_max_sync(0xffffffffu, (u32)nm);
+    int qn = 0;
+    for (int k = 0; k < kmax; k++) {
+        bool check = false;
+        Board g;
+        u32 gs = 0;
+        CountPrep pr;
+        if (k < nm) {
+            g = b;
+            gs = st;
+            make_move<1 - C>(g, gs, mv[k]);
+            pr = count_prep<C>(g);
+            check = prep_in_check<C>(pr);
+            if (!check) total += count_quiet<C, STRICT>(pr.s, gs, pr.pinned, pr.threat, pr.ksq);
+        }
+        const unsigned dm = __ballot_sync(0xffffffffu, check);
+        if (dm) {
+            if (check) {
+                const int slot = qn + __popc(dm & ((1u << lane) - 1u));
+                q_b[warp][slot] = g;
+                q_pin[warp][slot] = pr.pinned;
+                q_thr[warp][slot] = pr.threat;
+                q_st[warp][slot] = (uint8_t)gs;
+            }
+            qn += __popc(dm);
+            __syncwarp();
+            if (qn >= 32) {
+                const int slot = qn - 32 + lane;
+                const Board e = q_b[warp][slot];
+                const Sets es = derive<C>(e);
+                total += count_evasions<C, STRICT>(es, q_st[warp][slot], q_pin[warp][slot], q_thr[warp][slot],
+                                                   bit_index(es.kings & es.us));
+                qn -= 32;
+                __syncwarp();
+            }
+        }
+    }
+    if (lane < qn) {
+        const Board e = q_b[warp][lane];
+        const Sets es = derive<C>(e);
+        total += count_evasions<C, STRICT>(es, q_st[warp][lane], q_pin[warp][lane], q_thr[warp][lane],
+                                           bit_index(es.kings & es.us));
+    }
+    const u32 t = __reduce_add_sync(0xffffffffu, total);
+    const u32 c = __reduce_add_sync(0xffffffffu, counted);
+    if (lane == 0 && c) {
+        atomicAdd(counter, (unsigned long long)t);
+        atomicAdd(counter + 1, (unsigned long long)c);
+    }
+}
+
+}  // namespace pb

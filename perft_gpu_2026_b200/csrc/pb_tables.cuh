@@ -52,9 +52,9 @@ static bool fill_magic(Magic &m, int sq, u64 mul, const int (*dirs)[2], u32 offs
     int bits = popc(mask);
     m.mask = mask;
     m.magic = mul;
-    m.offset = offset;
+    m.base = offset;
     m.shift = 64 - bits;
-    m.pad = 0;
+    m.shift_hi = 32 - bits;
     u32 n = 1u << bits;
     for (u32 i = 0; i < n; i++) h_attacks[offset + i] = ~0ULL;
     u64 sub = 0;
@@ -70,6 +70,17 @@ static bool fill_magic(Magic &m, int sq, u64 mul, const int (*dirs)[2], u32 offs
 }
 
 }  // namespace tables_detail
+
+// Device copy of h_tab: magic slices point at their device addresses.
+inline Tables device_tables(const u64 *dev_attacks)
+{
+    Tables t = h_tab;
+    for (int sq = 0; sq < 64; sq++) {
+        t.rook[sq].base = (u64)(uintptr_t)(dev_attacks + h_tab.rook[sq].base);
+        t.bishop[sq].base = (u64)(uintptr_t)(dev_attacks + h_tab.bishop[sq].base);
+    }
+    return t;
+}
 
 // Builds h_tab / h_attacks.  Returns false if a multiplier is wrong.
 inline bool build_host_tables()

@@ -194,3 +194,15 @@ def test_autotune_picks_a_candidate():
     assert res["best"] in autotune.candidates()
     assert eng.get_tuning().as_dict()["leaf_threads"] == res["best"]["leaf_threads"]
     eng.close()
+
+
+@pytest.mark.parametrize("threads", [128, 256])
+def test_deferred_evasion_leaf(golden, threads):
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
+    eng.set_tuning(leaf_kernel=3, leaf_threads=threads)
+    for case in golden:
+        p = pg.parse_fen(case["fen"])
+        for d, want in enumerate(case["counts"], start=1):
+            assert eng.perft_position(p, d) == want, (case["name"], d)
+    assert eng.perft_position(pg.parse_fen(KIWIPETE), 6) == 8031647685
+    eng.close()
