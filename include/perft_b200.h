@@ -160,7 +160,10 @@ typedef struct {
     int leaf_threads;   /* CTA size of the one-edge-per-thread leaf: 128, 256 (default) or 512 */
     int gen_threads;    /* CTA size of the staged generator: 64 or 128 (default); stages 64 moves per thread */
     int leaf_fuse;      /* plies fused in the leaf kernel: 2 (default) or 1 (one more BFS level) */
-    int reserved[3];
+    int tt_replace;     /* device TT replacement: 1 = always overwrite (default, tt.h:60-70),
+                           2 = two-slot buckets, the larger subtree keeps the first slot;
+                           takes effect when the device tables are next sized */
+    int reserved[2];
 } pb_tuning;
 
 int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t);

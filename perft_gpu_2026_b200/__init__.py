@@ -87,11 +87,11 @@ class Tuning(ctypes.Structure):
 
     _fields_ = [("leaf_kernel", ctypes.c_int), ("leaf_blocks_per_sm", ctypes.c_int),
                 ("leaf_threads", ctypes.c_int), ("gen_threads", ctypes.c_int), ("leaf_fuse", ctypes.c_int),
-                ("reserved", ctypes.c_int * 3)]
+                ("tt_replace", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k in ("leaf_kernel", "leaf_blocks_per_sm", "leaf_threads", "gen_threads",
-                                              "leaf_fuse")}
+                                              "leaf_fuse", "tt_replace")}
 
 
 class PlanStats(ctypes.Structure):
@@ -370,8 +370,9 @@ class Engine:
         self._check(lib.pb_set_timing(self._h, int(enable)))
 
     def set_tuning(self, leaf_kernel: int = 0, leaf_blocks_per_sm: int = 0, leaf_threads: int = 0,
-                   gen_threads: int = 0, leaf_fuse: int = 0) -> None:
+                   gen_threads: int = 0, leaf_fuse: int = 0, tt_replace: int = 0) -> None:
         t = Tuning()
+        t.tt_replace = tt_replace
         t.leaf_kernel = leaf_kernel
         t.leaf_blocks_per_sm = leaf_blocks_per_sm
         t.leaf_threads = leaf_threads

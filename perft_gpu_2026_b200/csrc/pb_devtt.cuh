@@ -35,19 +35,20 @@ struct TTView {
     u64 *entries;  // SHALLOW: 2 words per slot, DEEP: 4 words per slot
     u64 slots;     // any size: the slot is the high word of lo * slots
     int kind;
+    int buckets;   // 0: one slot, always overwrite; 1: two-slot buckets, size priority
 };
 
 __device__ __forceinline__ u64 tt_slot(const TTView &t, u64 lo) { return __umul64hi(lo, t.slots); }
 
-__device__ __forceinline__ bool tt_probe(const TTView &t, const Hash128 &h, u64 *out)
+// Entry in slot `slot` matching the key?  (*count = its count; *used = slot holds anything)
+__device__ __forceinline__ bool tt_read(const TTView &t, u64 slot, const Hash128 &h, u64 *count, u64 *held)
 {
-    if (t.kind == TT_NONE) return false;
-    u64 slot = tt_slot(t, h.lo);
     if (t.kind == TT_SHALLOW) {
         u64 w0, w1;
         asm volatile("ld.global.v2.u64 {%0,%1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(t.entries + 2 * slot));
+        *held = (w1 & SHALLOW_COUNT_MASK) ? (w1 & SHALLOW_COUNT_MASK) - 1 : 0;
         if ((w0 ^ w1) == h.hi && ((w1 ^ (h.lo << 24)) & ~SHALLOW_COUNT_MASK) == 0 && (w1 & SHALLOW_COUNT_MASK)) {
-            *out = (w1 & SHALLOW_COUNT_MASK) - 1;
+            *count = (w1 & SHALLOW_COUNT_MASK) - 1;
             return true;
         }
         return false;
@@ -56,17 +57,16 @@ __device__ __forceinline__ bool tt_probe(const TTView &t, const Hash128 &h, u64 
     asm volatile("ld.global.v4.u64 {%0,%1,%2,%3}, [%4];"
                  : "=l"(w0), "=l"(w1), "=l"(w2), "=l"(w3)
                  : "l"(t.entries + 4 * slot));
+    *held = (w0 | w1 | w2 | w3) ? w2 : 0;
     if ((w0 ^ w2) == h.lo && (w1 ^ w2) == h.hi && (w3 ^ w2) == (h.lo ^ h.hi) && (w0 | w1 | w2 | w3)) {
-        *out = w2;
+        *count = w2;
         return true;
     }
     return false;
 }
 
-__device__ __forceinline__ void tt_store(const TTView &t, const Hash128 &h, u64 count)
+__device__ __forceinline__ void tt_write(const TTView &t, u64 slot, const Hash128 &h, u64 count)
 {
-    if (t.kind == TT_NONE) return;
-    u64 slot = tt_slot(t, h.lo);
     if (t.kind == TT_SHALLOW) {
         if (count + 1 > SHALLOW_COUNT_MASK) return;  // never truncate a count
         u64 w1 = (h.lo << 24) | (count + 1);
@@ -77,6 +77,37 @@ __device__ __forceinline__ void tt_store(const TTView &t, const Hash128 &h, u64 
     asm volatile("st.global.v4.u64 [%0], {%1,%2,%3,%4};" ::"l"(t.entries + 4 * slot), "l"(h.lo ^ count),
                  "l"(h.hi ^ count), "l"(count), "l"(h.lo ^ h.hi ^ count)
                  : "memory");
+}
+
+__device__ __forceinline__ bool tt_probe(const TTView &t, const Hash128 &h, u64 *out)
+{
+    if (t.kind == TT_NONE) return false;
+    u64 slot = tt_slot(t, h.lo), held;
+    if (!t.buckets) return tt_read(t, slot, h, out, &held);
+    slot &= ~1ULL;
+    return tt_read(t, slot, h, out, &held) || tt_read(t, slot + 1, h, out, &held);
+}
+
+// Always-overwrite (the reference's rule, tt.h:60-70), or with two-slot
+// buckets: a key already present is refreshed in place, otherwise the first
+// slot keeps the larger subtree and the second takes whatever is displaced
+// or stored.
+__device__ __forceinline__ void tt_store(const TTView &t, const Hash128 &h, u64 count)
+{
+    if (t.kind == TT_NONE) return;
+    u64 slot = tt_slot(t, h.lo);
+    if (!t.buckets) {
+        tt_write(t, slot, h, count);
+        return;
+    }
+    slot &= ~1ULL;
+    u64 c0, c1, held0, held1;
+    if (tt_read(t, slot, h, &c0, &held0)) return;
+    if (tt_read(t, slot + 1, h, &c1, &held1)) return;
+    if (count >= held0)
+        tt_write(t, slot, h, count);
+    else
+        tt_write(t, slot + 1, h, count);
 }
 
 struct TTViews {
@@ -94,6 +125,8 @@ struct DeviceTT {
     // budget_mb 0 = auto (a share of `free_bytes`).  Depth 2 and 3 get the
     // shallow format; the split gives the leaf table (depth 2) a quarter,
     // depth 3 a quarter and the rest to depths 4..max_depth-1.
+    int buckets = 0;
+
     int init(int budget_mb, size_t free_bytes, int max_depth, int verbose, std::string *err)
     {
         release();
@@ -108,7 +141,9 @@ struct DeviceTT {
             bool shallow = r <= 3;
             u64 esz = shallow ? 16 : 32;
             u64 slots = want / esz;
-            if (shallow && slots < (1ULL << 24)) continue;  // too small for key verification
+            // the stored 40 low bits of lo pin the key only while a slot (or a
+            // two-slot bucket) spans less than 2^40 values of lo
+            if (shallow && slots < (buckets ? (1ULL << 25) : (1ULL << 24))) continue;
             if (!shallow && slots < 1024) continue;
             void *p = nullptr;
             if (cudaMalloc(&p, slots * esz) != cudaSuccess) {
@@ -117,7 +152,7 @@ struct DeviceTT {
             }
             cudaMemset(p, 0, slots * esz);
             blocks.push_back(p);
-            views.v[r] = TTView{reinterpret_cast<u64 *>(p), slots, shallow ? TT_SHALLOW : TT_DEEP};
+            views.v[r] = TTView{reinterpret_cast<u64 *>(p), slots, shallow ? TT_SHALLOW : TT_DEEP, buckets};
             bytes += slots * esz;
             if (verbose)
                 printf("Device TT[%d]%s: %lluM entries (%llu MB)\n", r, shallow ? " (shallow)" : "",
@@ -139,7 +174,7 @@ struct DeviceTT {
         views = TTViews{};
         bytes = 0;
     }
-    TTView at(int r) const { return (r >= 0 && r < TT_MAX_DEPTH) ? views.v[r] : TTView{nullptr, 0, TT_NONE}; }
+    TTView at(int r) const { return (r >= 0 && r < TT_MAX_DEPTH) ? views.v[r] : TTView{nullptr, 0, TT_NONE, 0}; }
 };
 
 // ---------------------------------------------------------------- TT-mode kernels

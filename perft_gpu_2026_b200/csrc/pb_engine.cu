@@ -70,7 +70,7 @@ struct pb_ctx {
     u64 *h_pinned = nullptr;  // pinned host words for readbacks
     int launch_depth = 0;
     bool timing = false;
-    pb_tuning tuning{1, 0, 256, 128, 2, {0, 0, 0}};
+    pb_tuning tuning{1, 0, 256, 128, 2, 1, {0, 0}};
     int num_sms = 0;
     uint16_t *spill = nullptr;  // cooperative-leaf spill area (device)
     size_t spill_blocks = 0;
@@ -371,6 +371,7 @@ int ensure_dtt(pb_ctx *ctx, int max_r)
     if (ctx->dtt.ready() && ctx->dtt_max_depth >= max_r) return PB_OK;
     // (re)size for depths 2..max_r; a deeper call than prepared drops the
     // current contents, which only costs hits
+    ctx->dtt.buckets = ctx->tuning.tt_replace == 2 ? 1 : 0;
     ctx->dtt.init(ctx->opts.device_tt_mb, ctx->dtt_free_bytes, max_r, ctx->opts.verbose, &ctx->err);
     ctx->dtt_max_depth = max_r;
     return PB_OK;
@@ -1485,6 +1486,14 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
     if (t->leaf_fuse) {
         if (t->leaf_fuse != 1 && t->leaf_fuse != 2) return PB_ERR_ARG;
         ctx->tuning.leaf_fuse = t->leaf_fuse;
+    }
+    if (t->tt_replace) {
+        if (t->tt_replace != 1 && t->tt_replace != 2) return PB_ERR_ARG;
+        if (t->tt_replace != ctx->tuning.tt_replace) {
+            ctx->tuning.tt_replace = t->tt_replace;
+            ctx->dtt.release();  // resized (and re-laid-out) on the next TT call
+            ctx->dtt_max_depth = 0;
+        }
     }
     return PB_OK;
 }

@@ -1,6 +1,7 @@
 // perft_cli.cpp - the perft_gpu command line on top of the C ABI.
 //
-//   perft_gpu <fen> <depth> [<launchdepth>] [-nott] [-dtt <MB>] [-htt <MB>] [-ld <N>] [-cpu] [-strict]
+//   perft_gpu <fen> <depth> [<launchdepth>] [-nott] [-dtt <MB>] [-htt <MB>] [-ld <N>] [-cpu] [-strict] [-json]
+//   perft_gpu -batch <file> [<depth>] [-cpu] [-strict] [-json]
 //
 // Same surface and output as the reference program (perft.cu:13-186):
 // flags may appear anywhere, a third positional argument is the launch depth,
@@ -8,10 +9,19 @@
 //   "\nPerft(%02d): <count>, time: <s> seconds, nps: <n>\n"
 // (launcher.cu:732-735).  -strict is new: it counts the two cases where the
 // reference's move counting merges two moves (see include/perft_b200.h).
+// -json adds one JSON object per depth after the usual line.  -batch runs a
+// file of positions, one per line: a FEN followed by optional ";D<k> <count>"
+// expected counts (EPD-style); every depth up to the largest listed (or the
+// <depth> argument) runs as one batched GPU pass over all positions, and
+// mismatches against the listed counts are reported.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+#include <chrono>
+#include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -52,9 +62,106 @@ static void print_depth(int d, pb_u128 v, double secs)
     fflush(stdout);
 }
 
+static void print_json(int d, pb_u128 v, double secs)
+{
+    printf("{\"depth\": %d, \"nodes\": \"%s\", \"seconds\": %.9g, \"nps\": %.6g}\n", d, u128_text(v).c_str(), secs,
+           secs > 0 ? u128_double(v) / secs : 0.0);
+    fflush(stdout);
+}
+
+struct BatchLine {
+    std::string fen;
+    std::vector<std::pair<int, unsigned long long>> expect;
+};
+
+static int run_batch(const std::string &path, int depth_arg, bool cpu, bool json, pb_opts opts)
+{
+    std::ifstream in(path);
+    if (!in) {
+        fprintf(stderr, "cannot open %s\n", path.c_str());
+        return 1;
+    }
+    std::vector<BatchLine> lines;
+    std::vector<pb_pos> roots;
+    std::string line;
+    int maxd = 0;
+    while (std::getline(in, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        BatchLine bl;
+        size_t semi = line.find(';');
+        bl.fen = line.substr(0, semi);
+        while (semi != std::string::npos) {
+            size_t next = line.find(';', semi + 1);
+            std::string item = line.substr(semi + 1, next == std::string::npos ? std::string::npos : next - semi - 1);
+            std::istringstream is(item);
+            std::string tag;
+            unsigned long long cnt = 0;
+            if (is >> tag >> cnt && tag.size() >= 2 && (tag[0] == 'D' || tag[0] == 'd'))
+                bl.expect.push_back({atoi(tag.c_str() + 1), cnt});
+            semi = next;
+        }
+        pb_pos p;
+        if (pb_parse_fen(bl.fen.c_str(), &p) != PB_OK) {
+            fprintf(stderr, "invalid FEN in %s: %s\n", path.c_str(), bl.fen.c_str());
+            return 1;
+        }
+        for (auto &e : bl.expect) maxd = std::max(maxd, e.first);
+        lines.push_back(bl);
+        roots.push_back(p);
+    }
+    int depth = depth_arg > 0 ? depth_arg : (maxd > 0 ? maxd : 1);
+    pb_ctx *ctx = nullptr;
+    opts.use_tt = 0;
+    if (pb_create(cpu ? -1 : 0, &opts, &ctx) != PB_OK) {
+        fprintf(stderr, "init failed\n");
+        return 1;
+    }
+    int n = (int)roots.size(), bad = 0;
+    std::vector<uint64_t> counts(n);
+    std::vector<int> depths(n);
+    for (int d = 1; d <= depth; d++) {
+        auto t0 = std::chrono::steady_clock::now();
+        int rc;
+        if (cpu) {
+            rc = PB_OK;
+            for (int i = 0; i < n && rc == PB_OK; i++) rc = pb_perft_cpu(ctx, &roots[i], d, &counts[i]);
+        } else {
+            for (int i = 0; i < n; i++) depths[i] = d;
+            rc = pb_perft_batch(ctx, roots.data(), depths.data(), n, counts.data());
+        }
+        double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (rc != PB_OK) {
+            fprintf(stderr, "error: %s\n", pb_last_error(ctx));
+            pb_destroy(ctx);
+            return 1;
+        }
+        pb_u128 total{0, 0};
+        for (int i = 0; i < n; i++) {
+            unsigned long long old = total.lo;
+            total.lo += counts[i];
+            if (total.lo < old) total.hi++;
+            const char *mark = "";
+            for (auto &e : lines[i].expect)
+                if (e.first == d && e.second != counts[i]) {
+                    mark = "  MISMATCH";
+                    bad++;
+                }
+            printf("pos %d Perft(%02d): %llu%s\n", i + 1, d, (unsigned long long)counts[i], mark);
+        }
+        printf("\nBatch Perft(%02d): %s over %d positions, time: %g seconds, nps: %llu\n", d, u128_text(total).c_str(), n,
+               secs, (unsigned long long)(secs > 0 ? u128_double(total) / secs : 0));
+        if (json) print_json(d, total, secs);
+        fflush(stdout);
+    }
+    printf("batch: %d positions, %d mismatches\n", n, bad);
+    pb_destroy(ctx);
+    return bad ? 2 : 0;
+}
+
 int main(int argc, char **argv)
 {
-    bool cpu = false;
+    bool cpu = false, json = false;
+    std::string batch_file;
     pb_opts opts;
     pb_default_opts(&opts);
     std::vector<std::string> pos;
@@ -63,11 +170,14 @@ int main(int argc, char **argv)
         if (a == "-cpu") cpu = true;
         else if (a == "-nott") opts.use_tt = 0;
         else if (a == "-strict") opts.strict = 1;
+        else if (a == "-json") json = true;
+        else if (a == "-batch" && i + 1 < argc) batch_file = argv[++i];
         else if (a == "-ld" && i + 1 < argc) opts.launch_depth = atoi(argv[++i]);
         else if (a == "-dtt" && i + 1 < argc) opts.device_tt_mb = atoi(argv[++i]);
         else if (a == "-htt" && i + 1 < argc) opts.host_tt_mb = atoi(argv[++i]);
         else pos.push_back(a);
     }
+    if (!batch_file.empty()) return run_batch(batch_file, pos.empty() ? 0 : atoi(pos[0].c_str()), cpu, json, opts);
     std::string fen = "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1";
     int max_depth = 10;
     if (pos.size() >= 2) {
@@ -102,6 +212,7 @@ int main(int argc, char **argv)
                 return 1;
             }
             print_depth(d, v, secs);
+            if (json) print_json(d, v, secs);
         }
         pb_destroy(ctx);
         return 0;
@@ -130,6 +241,7 @@ int main(int argc, char **argv)
             return 1;
         }
         print_depth(d, v, secs);
+        if (json) print_json(d, v, secs);
     }
     pb_destroy(ctx);
     return 0;

@@ -69,3 +69,19 @@ def test_tt_strict_mode(oracle):
     p = pg.parse_fen(fen)
     assert [eng.perft_position(p, d) for d in (3, 4, 5)] == [oracle.perft(fen, d, True) for d in (3, 4, 5)]
     eng.close()
+
+
+def test_size_priority_buckets_stay_exact():
+    eng = pg.Engine(device=0, use_tt=True, arena_bytes=2 << 30, device_tt_mb=2048, host_tt_mb=256)
+    eng.set_tuning(tt_replace=2)
+    p = pg.parse_fen(START)
+    assert [eng.perft_position(p, d) for d in (5, 6, 7)] == [4865609, 119060324, 3195901860]
+    ref = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
+    for q, d in [(pg.parse_fen(KIWIPETE), 6), (pg.config_position(4, 1), 7)]:
+        assert eng.perft_position(q, d) == ref.perft_position(q, d)
+    ref.close()
+    small = pg.Engine(device=0, use_tt=True, arena_bytes=1 << 30, device_tt_mb=1, host_tt_mb=1)
+    small.set_tuning(tt_replace=2)
+    assert small.perft_position(pg.parse_fen(KIWIPETE), 5) == 193690690
+    small.close()
+    eng.close()

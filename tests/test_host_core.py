@@ -111,3 +111,24 @@ def test_cpu_cli_output_format():
     assert [l.split(",")[0] for l in lines] == ["Perft(01): 20", "Perft(02): 400", "Perft(03): 8902",
                                                  "Perft(04): 197281"]
     assert all(" seconds" in l for l in lines)
+
+
+def test_cli_batch_file_and_json(tmp_path):
+    import json
+    import os
+    import subprocess
+    cli = os.path.join(os.path.dirname(pg.__file__), "perft_gpu")
+    f = tmp_path / "pos.epd"
+    f.write_text("# comment\n"
+                 "rnbqkbnr/pppppppp/8/8/8/8/PPPPPPPP/RNBQKBNR w KQkq - 0 1 ;D1 20 ;D2 400 ;D3 8902\n"
+                 "2n4k/1P1P4/8/8/8/8/8/4K3 w - - 0 1 ;D1 17 ;D2 93\n")
+    out = subprocess.run([cli, "-batch", str(f), "-cpu", "-json"], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    js = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert [j["nodes"] for j in js] == ["37", "493", "10523"]
+    assert "0 mismatches" in out.stdout
+    f.write_text("2n4k/1P1P4/8/8/8/8/8/4K3 w - - 0 1 ;D1 21\n")  # the exact count, not the reference's
+    out = subprocess.run([cli, "-batch", str(f), "-cpu"], capture_output=True, text=True)
+    assert out.returncode == 2 and "MISMATCH" in out.stdout
+    out = subprocess.run([cli, "-batch", str(f), "-cpu", "-strict"], capture_output=True, text=True)
+    assert out.returncode == 0
