@@ -229,7 +229,13 @@ def main():
     elif not args.no_autotune:
         from perft_gpu_2026_b200 import autotune
 
-        tuning = autotune.load_or_tune(eng, local)["best"]
+        # rank 0 tunes (or reads the cache); the others read what it wrote
+        if rank == 0:
+            tuning = autotune.load_or_tune(eng, local)["best"]
+        if dist:
+            dist.barrier()
+        if rank != 0:
+            tuning = autotune.load_or_tune(eng, local)["best"]
     eng.set_timing(True)
 
     # shard: depth-2 subtrees round-robin over ranks (one rank: the whole root)
