@@ -18,6 +18,8 @@ Printed JSON line (rank 0):
   roofline the leaf kernel against the integer-issue roofline
   cpu_baseline  the reference's own -cpu path (oracle/_ref) on this host's
            cores, one process per core over a sample of depth-2 subtrees
+  positions  (one GPU) positions/s on 4096 uneven roots at perft 5: plain
+           per-root calls, count-then-allocate batch, learned planner
 With --gpus N > 1 (torchrun, one process per GPU) the depth-2 subtrees of the
 root are split over the ranks (strong scaling: total work fixed); the only
 exchange is one all-reduce of the per-rank counts.
@@ -160,6 +162,52 @@ def cpu_reference_sample(pg, root, depth, max_seconds=20.0, cores=None):
             "nodes": nodes, "seconds": wall}
 
 
+def positions_section(pg, eng, reps):
+    """Positions/s on 4096 uneven roots (playouts of 6..40 plies, splitmix64
+    seed 2), perft 5 each, three ways through the public API (roots in host
+    memory, counts read back, host wall clock): one plain call per root, one
+    count-then-allocate batched call, and the learned planner (network trained
+    here by the library's own kernels on 2^18 playout positions of 0..60 plies,
+    seed 3, labelled with exact perft 1..4).  All three must agree."""
+    import numpy as np
+    from perft_gpu_2026_b200 import scheduler
+
+    roots = pg.uneven_roots(4096, 6, 40, seed=2)
+    depths = [5] * len(roots)
+    t0 = time.perf_counter()
+    pos, y, _ = scheduler.make_training_set(eng, 1 << 18)
+    eng.mlp_init(seed=1, out_bias=list(y.mean(0)))
+    loss = eng.mlp_train(pos, y, epochs=12, batch=4096, lr=2e-3)
+    train_s = time.perf_counter() - t0
+    truth = np.log2(1.0 + scheduler.label(eng, roots))
+    mae = np.abs(eng.mlp_predict(roots) - truth).mean(0).tolist()
+
+    def timed(fn):
+        fn()  # warm-up (graph capture, arena growth)
+        best, out = None, None
+        for _ in range(reps):
+            t = time.perf_counter()
+            out = fn()
+            dt = time.perf_counter() - t
+            best = dt if best is None else min(best, dt)
+        return out, best
+
+    plain, t_plain = timed(lambda: [eng.perft_position(r, 5) for r in roots])
+    batched, t_batched = timed(lambda: eng.perft_batch(roots, depths))
+    (learned, plan), t_learned = timed(lambda: eng.perft_batch_planned(roots, depths))
+    assert plain == batched == list(learned), "batched or planned counts differ from the plain path"
+    n = len(roots)
+    return {"workload": "4096 uneven roots (6..40-ply playouts, seed 2), perft 5 each, no TT",
+            "unit": "positions/s", "timing": "host wall clock around the public call, best of "
+                                             f"{reps} after one warm-up",
+            "nodes": int(sum(plain)), "plain": n / t_plain, "batched": n / t_batched, "learned": n / t_learned,
+            "learned_vs_plain": t_plain / t_learned, "batched_vs_plain": t_plain / t_batched,
+            "plan": {"batches": plan.batches, "graph_batches": plan.graph_batches, "retries": plan.retries,
+                     "split_roots": plan.split_roots},
+            "scheduler": {"train_positions": len(pos), "train_mse": loss, "train_s": train_s,
+                          "mae_log2_perft1_4_on_roots": mae}}
+
+
 def run_reference_arm(args):
     import perft_gpu_2026_b200 as pg
 
@@ -199,6 +247,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--leaf-kernel", type=int, default=0, help="1 = edge per thread, 2 = cooperative (0 = engine default)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default launch parameters")
+    ap.add_argument("--no-positions", action="store_true", help="skip the batched-roots positions/s section")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -329,6 +378,8 @@ def main():
                         "h2d_bytes_per_step": int(results[0][5]), "d2h_bytes_per_step": int(results[0][6]),
                         "timing": "host wall clock around pb_perft_position"},
                 "gpu_launches": int(kernels), "clocks": clocks, "roofline": roofline}
+        if world == 1 and not args.no_positions:
+            line["positions"] = positions_section(pg, eng, reps=min(args.steps, 3))
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_reference_sample(pg, root, depth, max_seconds=15.0)
             if cb:

@@ -128,7 +128,8 @@ inline bool parse_fen(const char *fen, pb_pos *out)
     {
         Sets s = color == WHITE ? derive<BLACK>(b) : derive<WHITE>(b);  // sets from the other side's view
         u64 their_king = s.kings & s.us;
-        u64 att = color == WHITE ? enemy_attacks<BLACK>(s, 0) : enemy_attacks<WHITE>(s, 0);
+        int tk = bit_index(their_king);
+        u64 att = color == WHITE ? enemy_attacks<BLACK>(s, 0, tk) : enemy_attacks<WHITE>(s, 0, tk);
         if (att & their_king) return false;
     }
     for (int k = 0; k < 4; k++) out->bb[k] = b.bb[k];

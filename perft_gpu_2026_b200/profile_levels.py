@@ -21,9 +21,10 @@ def main():
     ap.add_argument("--roots", type=int, default=1 << 18)
     ap.add_argument("--depth", type=int, default=4)
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--arena-gb", type=int, default=24)
     args = ap.parse_args()
     roots = [p for p in pg.random_playouts(3, args.roots, 0, 60) if pg.count_moves(p, True) > 0]
-    eng = pg.Engine(device=0, use_tt=False, arena_bytes=24 << 30)
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=args.arena_gb << 30)
     eng.set_timing(True)
     for _ in range(args.reps):
         t = time.perf_counter()
