@@ -423,13 +423,130 @@ template <int C> PB_HD CountPrep count_prep(const Board &b)
 }
 template <int C> PB_HD bool prep_in_check(const CountPrep &p) { return (p.threat >> p.ksq) & 1; }
 
-// Number of legal moves (countMoves, MoveGeneratorBitboard.h:1700-1943).
+// Number of legal moves (countMoves, MoveGeneratorBitboard.h:1700-1943, and
+// countMovesOutOfCheck, :1564-1694, for a side in check).
+//
+// One code path for both cases, so a warp whose lanes disagree on being in
+// check does not run two count routines one after the other: every non-king
+// move must end on `safe` (all squares when not in check; the checker and
+// the squares between it and the king in single check; none in double
+// check), pinned pieces and castling are skipped in check, and the in-check
+// conventions of the out-of-check counter are kept (promotions counted per
+// capture direction, one en-passant capture of a checking pawn however many
+// pawns can take it).  Equal to count_quiet / count_evasions.  On the GPU a
+// group of lanes none of which is in check takes count_quiet, which skips
+// the masking.
 template <int C, bool STRICT>
 PB_HD u32 count_moves(const Board &b, u32 state)
 {
-    CountPrep p = count_prep<C>(b);
-    if (prep_in_check<C>(p)) return count_evasions<C, STRICT>(p.s, state, p.pinned, p.threat, p.ksq);
-    return count_quiet<C, STRICT>(p.s, state, p.pinned, p.threat, p.ksq);
+    const CountPrep p = count_prep<C>(b);
+    const Sets &s = p.s;
+    const int ksq = p.ksq;
+    const u64 king = 1ULL << ksq;
+    const bool check = (p.threat & king) != 0;
+#ifdef __CUDA_ARCH__
+    // no lane of the converged group in check: the leaner not-in-check path
+    if (!__any_sync(__activemask(), check)) return count_quiet<C, STRICT>(s, state, p.pinned, p.threat, ksq);
+#endif
+    u64 safe = ~0ULL, checkers = 0;
+    if (check) {
+        checkers = (cap_west<C>(king) | cap_east<C>(king)) & s.pawns & s.them;
+        checkers |= knight_att(ksq) & s.knights & s.them;
+        checkers |= bishop_att(ksq, s.occ) & s.bq & s.them;
+        checkers |= rook_att(ksq, s.occ) & s.rq & s.them;
+        safe = more_than_one(checkers) ? 0 : checkers | between(ksq, bit_index(checkers));
+    }
+    const u64 pinned = check ? 0 : p.pinned;  // in check a pinned piece never moves
+    const u64 movable = s.us & ~p.pinned;
+    const u64 er = s.rq & s.them;
+    const u64 empty = ~s.occ;
+    const u64 my_pawns = s.pawns & s.us;
+    u32 n = popc(king_att(ksq) & ~(p.threat | s.us));
+
+    u64 ept = ep_target<C>(state);
+    if (ept) {
+        u64 victim = push1<1 - C>(ept);
+        if (!check || victim == checkers) {
+            u64 src = (east1(victim) | west1(victim)) & (check ? my_pawns & movable : my_pawns);
+            u32 e = 0;
+            while (src) {
+                int psq = lsb(src);
+                u64 pawn = 1ULL << psq;
+                if (pawn & pinned) {
+                    if (ept & line_through(psq, ksq)) e++;
+                } else {
+                    u64 occ2 = s.occ ^ victim ^ pawn;
+                    u64 rank = RANK1 << (ksq & 56);
+                    if (!(rook_att(ksq, occ2) & er & rank)) e++;
+                }
+                src &= src - 1;
+            }
+            n += (check && !STRICT && e > 1u) ? 1u : e;
+        }
+    }
+
+    u64 pp = my_pawns & pinned;
+    while (pp) {
+        int psq = lsb(pp);
+        u64 pawn = 1ULL << psq;
+        u64 ln = line_through(psq, ksq);
+        u64 d = push1<C>(pawn) & ln & empty;
+        if (d) {
+            n++;
+            if (push1<C>(d & double_push_rank<C>()) & empty) n++;
+        }
+        d = (cap_west<C>(pawn) | cap_east<C>(pawn)) & ln & s.them;
+        if (d) n += (d & PROMO_RANKS) ? 4 : 1;
+        pp &= pp - 1;
+    }
+
+    const u64 fp = my_pawns & movable;
+    const u64 p1 = push1<C>(fp) & empty;
+    const u64 s1 = p1 & safe;
+    n += popc(push1<C>(p1 & double_push_rank<C>()) & empty & safe);
+    const u64 cw = cap_west<C>(fp) & s.them & safe, ce = cap_east<C>(fp) & s.them & safe;
+    constexpr u64 RANK7 = C == WHITE ? 0x00FF000000000000ULL : 0x000000000000FF00ULL;
+    if (!(fp & RANK7)) {
+        n += popc(s1) + popc(cw) + popc(ce);
+    } else {
+        u64 promos = s1 & PROMO_RANKS;
+        u64 pw = cw & PROMO_RANKS, pe = ce & PROMO_RANKS;
+        n += popc(s1 ^ promos) + popc(cw ^ pw) + popc(ce ^ pe);
+        if (STRICT || check)
+            n += 4 * (popc(promos) + popc(pw) + popc(pe));
+        else
+            n += 4 * popc(promos | pw | pe);
+    }
+
+    u32 castle = C == WHITE ? (state & 3) : ((state >> 2) & 3);
+    if (castle && !check) {
+        constexpr u64 KS = C == WHITE ? 0x60ULL : 0x6000000000000000ULL;
+        constexpr u64 QS_EMPTY = C == WHITE ? 0x0EULL : 0x0E00000000000000ULL;
+        constexpr u64 QS_SAFE = C == WHITE ? 0x0CULL : 0x0C00000000000000ULL;
+        if ((castle & 1) && !(KS & (s.occ | p.threat))) n++;
+        if ((castle & 2) && !(QS_EMPTY & s.occ) && !(QS_SAFE & p.threat)) n++;
+    }
+
+    const u64 targets = ~s.us & safe;
+    u64 kn = s.knights & movable;
+    while (kn) {
+        n += popc(knight_att(lsb(kn)) & targets);
+        kn &= kn - 1;
+    }
+    for (u64 bs = s.bq & movable; bs; bs &= bs - 1) n += popc(bishop_att(lsb(bs), s.occ) & targets);
+    for (u64 rs = s.rq & movable; rs; rs &= rs - 1) n += popc(rook_att(lsb(rs), s.occ) & targets);
+    if (pinned & (s.bq | s.rq)) {
+        // a pinned slider moves only along the line through its king
+        for (u64 bs = s.bq & s.us & pinned; bs; bs &= bs - 1) {
+            int sq = lsb(bs);
+            n += popc(bishop_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
+        }
+        for (u64 rs = s.rq & s.us & pinned; rs; rs &= rs - 1) {
+            int sq = lsb(rs);
+            n += popc(rook_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
+        }
+    }
+    return n;
 }
 
 // ---------------------------------------------------------------- generation
