@@ -81,6 +81,7 @@ struct Tables {
     // squares c..g of its back rank.
     u64 rook_reach[64];
     u64 bishop_reach[64];
+    u64 knight_reach[64];  // squares from which a knight attacks that zone
 };
 constexpr int ATTACK_TABLE_SIZE = 107648;  // sum over squares of 2^bits (rook 102400 + bishop 5248)
 
@@ -149,10 +150,11 @@ PB_HD u64 magic_lookup(const Magic *e, u64 occ)
 #ifdef __CUDA_ARCH__
     // bits <= 12, so the index lies in the high word of the product: one
     // 32-bit shift instead of a 64-bit variable shift
-    ulonglong2 mm = __ldg(reinterpret_cast<const ulonglong2 *>(e));
-    ulonglong2 bs = __ldg(reinterpret_cast<const ulonglong2 *>(&e->base));
-    u32 hi = (u32)(((occ & mm.x) * mm.y) >> 32);
-    return __ldg(reinterpret_cast<const u64 *>(bs.x) + (hi >> (u32)bs.y));
+    // the whole 32-byte entry in one 256-bit load
+    u64 mask, mul, base, sh;
+    asm("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];" : "=l"(mask), "=l"(mul), "=l"(base), "=l"(sh) : "l"(e));
+    u32 hi = (u32)(((occ & mask) * mul) >> 32);
+    return __ldg(reinterpret_cast<const u64 *>(base) + (hi >> (u32)sh));
 #else
     u64 idx = ((occ & e->mask) * e->magic) >> e->shift;
     return h_attacks[e->base + (u32)idx];
@@ -168,6 +170,7 @@ PB_HD u64 rook_empty(int sq) { return ldg64(&PB_TAB.rook_empty[sq]); }
 PB_HD u64 bishop_empty(int sq) { return ldg64(&PB_TAB.bishop_empty[sq]); }
 PB_HD u64 rook_reach(int ksq) { return ldg64(&PB_TAB.rook_reach[ksq]); }
 PB_HD u64 bishop_reach(int ksq) { return ldg64(&PB_TAB.bishop_reach[ksq]); }
+PB_HD u64 knight_reach(int ksq) { return ldg64(&PB_TAB.knight_reach[ksq]); }
 
 // Knight attacks of a whole set by shifts (no per-piece loop).
 PB_HD u64 knights_bulk(u64 n)
@@ -242,8 +245,8 @@ template <int C> PB_HD u64 enemy_attacks(const Sets &s, u64 my_king, int ksq)
 {
     u64 ep = s.pawns & s.them;
     u64 a = cap_west<1 - C>(ep) | cap_east<1 - C>(ep);
-    a |= knights_bulk(s.knights & s.them);
     a |= king_att(bit_index(s.kings & s.them));
+    for (u64 kn = s.knights & s.them & knight_reach(ksq); kn; kn &= kn - 1) a |= knight_att(lsb(kn));
     u64 occ = s.occ ^ my_king;
     u64 b = s.bq & s.them & bishop_reach(ksq);
     while (b) {

@@ -145,13 +145,15 @@ inline bool build_host_tables()
         u64 zone = h_tab.king[k] | (1ULL << k);
         if (k == 4) zone |= 0x7CULL;                   // c1..g1
         if (k == 60) zone |= 0x7CULL << 56;            // c8..g8
-        u64 rr = 0, br = 0;
+        u64 rr = 0, br = 0, nr = 0;
         for (int sq = 0; sq < 64; sq++) {
             if (h_tab.rook_empty[sq] & zone) rr |= 1ULL << sq;
             if (h_tab.bishop_empty[sq] & zone) br |= 1ULL << sq;
+            if (h_tab.knight[sq] & zone) nr |= 1ULL << sq;
         }
         h_tab.rook_reach[k] = rr;
         h_tab.bishop_reach[k] = br;
+        h_tab.knight_reach[k] = nr;
     }
     u32 offset = 0;
     for (int sq = 0; sq < 64; sq++) {
