@@ -224,8 +224,8 @@ int pb_perft_batch_planned(pb_ctx *ctx, const pb_pos *roots, const int *depths, 
  * scratch (tile status words, ticket, error word) is a fixed device array
  * inside the library, so the call makes no cudaMalloc/cudaFree and no
  * allocating library call.
- *   - n is limited to 8,388,608 counts (4096 tiles of 2048); larger n returns
- *     PB_ERR_ARG without touching the GPU.
+ *   - n is limited to 8,388,608 counts (the array's status words cover that
+ *     many scan tiles); larger n returns PB_ERR_ARG without touching the GPU.
  *   - Runs on `stream` (NULL = default stream) of the current device and waits
  *     for it before returning; n == 0 returns PB_OK and writes nothing.
  *   - The first call on a device looks up the array's device address (set-up);

@@ -1289,7 +1289,9 @@ int estimate_launch_depth(pb_ctx *ctx, const Board &b, u32 st, int c)
 // the caller or the engine allocates.  Every GPU that loads the library holds
 // it (34 KB) until the process exits.
 constexpr u64 NOALLOC_SCAN_TILES = 4096;                              // status words
-constexpr u64 NOALLOC_SCAN_MAX_ITEMS = NOALLOC_SCAN_TILES * SCAN_TILE;  // 8,388,608 counts
+constexpr u64 NOALLOC_SCAN_MAX_ITEMS = 8388608;                      // counts per call
+static_assert((NOALLOC_SCAN_MAX_ITEMS + SCAN_TILE - 1) / SCAN_TILE <= NOALLOC_SCAN_TILES,
+              "the status words of the largest allowed scan must fit the fixed array");
 static __device__ __align__(256) u64 g_noalloc_scratch[NOALLOC_SCAN_TILES + 32];
 
 // Device address of g_noalloc_scratch per device, resolved once per device

@@ -75,8 +75,12 @@ __global__ void __launch_bounds__(256) k_expand_count(const Board *__restrict__ 
 // grand total lands in *total.  Tile status words: [63:62] flag (1 = tile
 // aggregate, 2 = inclusive prefix), [61:0] value.  Tiles are taken in launch
 // order from an atomic ticket so every predecessor is already resident.
+// 32 counts per thread: the scan is bound by each CTA's load -> look-back ->
+// store latency, so a larger tile moves more bytes per round trip (measured
+// on B200: 8 -> 16 -> 32 counts per thread = 2.3 -> 2.9 -> 3.4 TB/s at 400 M
+// counts; 64, or 512 threads, gain nothing more).
 constexpr int SCAN_THREADS = 256;
-constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_ITEMS = 32;  // a multiple of 8
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr u64 ST_AGG = 1ULL << 62, ST_PREFIX = 2ULL << 62, ST_VALUE = (1ULL << 62) - 1;
 constexpr u32 SCAN_SPIN_LIMIT = 1u << 22;
@@ -92,24 +96,77 @@ __device__ __forceinline__ u64 ld_acquire(const u64 *p)
     return v;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan(const u32 *__restrict__ in, u64 n, u64 *__restrict__ out,
-                                                       u64 *__restrict__ status, u32 *__restrict__ ticket,
-                                                       u64 *__restrict__ total, u32 *__restrict__ err)
+// Exclusive prefix of `tile` by decoupled look-back, run by one whole warp:
+// each step reads the status words of 32 predecessors at once, adds every
+// aggregate up to the nearest inclusive prefix, and retries while one of
+// those is not yet published.  Publishes the tile's aggregate first and its
+// inclusive prefix last.  Every lane returns the same value.  A wait longer
+// than SCAN_SPIN_LIMIT rounds sets DEVERR_SCAN_TIMEOUT and gives up.
+__device__ __forceinline__ u64 scan_lookback(u64 *status, u32 tile, u64 block_total, u32 *err)
 {
-    __shared__ u32 s_tile;
+    const int lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) st_release(status, ST_PREFIX | block_total);
+        return 0;
+    }
+    if (lane == 0) st_release(status + tile, ST_AGG | block_total);
+    u64 excl = 0;
+    long long p = (long long)tile - 1;
+    u32 spins = 0;
+    while (true) {
+        const long long q = p - lane;
+        const u64 w = q >= 0 ? ld_acquire(status + q) : ST_PREFIX;
+        const u32 flag = (u32)(w >> 62);
+        const unsigned not_ready = __ballot_sync(0xffffffffu, flag == 0);
+        const unsigned prefix = __ballot_sync(0xffffffffu, flag == 2);
+        // lanes from the nearest predecessor up to the nearest inclusive prefix
+        const unsigned upto = prefix ? (prefix & (0u - prefix)) * 2u - 1u : 0xffffffffu;
+        if (not_ready & upto) {
+            if (++spins > SCAN_SPIN_LIMIT) {
+                if (lane == 0) atomicOr(err, DEVERR_SCAN_TIMEOUT);
+                break;
+            }
+            continue;
+        }
+        u64 v = ((upto >> lane) & 1u) ? (w & ST_VALUE) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if (prefix) break;
+        p -= 32;
+    }
+    if (lane == 0) st_release(status + tile, ST_PREFIX | (excl + block_total));
+    return excl;
+}
+
+// One tile of the scan: SCAN_ITEMS consecutive counts per thread, read and
+// written with 256-bit accesses when both arrays are 32-byte aligned (the
+// engine's arena always is; callers' pointers may not be).
+__device__ __forceinline__ void scan_tile(const u32 *__restrict__ in, u64 n, u64 *__restrict__ out, u64 *status,
+                                          u32 tile, u64 *__restrict__ total, u32 *__restrict__ err)
+{
+    static_assert(SCAN_ITEMS % 8 == 0, "the vector path moves counts in 32-byte groups of 8");
     __shared__ u64 s_warp[SCAN_THREADS / 32];
     __shared__ u64 s_exclusive;
-    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
-    __syncthreads();
-    const u32 tile = s_tile;
     const u64 base = (u64)tile * SCAN_TILE + (u64)threadIdx.x * SCAN_ITEMS;
+    const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 31) == 0 &&
+                     base + SCAN_ITEMS <= n;
     u32 v[SCAN_ITEMS];
+    if (vec) {
+#pragma unroll
+        for (int g = 0; g < SCAN_ITEMS; g += 8) {
+            u64 a, b, c, d;
+            asm("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(in + base + g));
+            v[g + 0] = (u32)a, v[g + 1] = (u32)(a >> 32), v[g + 2] = (u32)b, v[g + 3] = (u32)(b >> 32);
+            v[g + 4] = (u32)c, v[g + 5] = (u32)(c >> 32), v[g + 6] = (u32)d, v[g + 7] = (u32)(d >> 32);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; k++) v[k] = (base + k < n) ? in[base + k] : 0u;
+    }
     u64 local = 0;
 #pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-        v[k] = (base + k < n) ? in[base + k] : 0u;
-        local += v[k];
-    }
+    for (int k = 0; k < SCAN_ITEMS; k++) local += v[k];
     // block-wide exclusive scan of the per-thread sums
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     u64 x = local;
@@ -128,51 +185,58 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(const u32 *__restrict__ i
             if (lane >= o) w += y;
         }
         if (lane < SCAN_THREADS / 32) s_warp[lane] = w;
-    }
-    __syncthreads();
-    const u64 block_total = s_warp[SCAN_THREADS / 32 - 1];
-    u64 thread_excl = x - local + (warp ? s_warp[warp - 1] : 0);
-
-    if (threadIdx.x == 0) {
-        u64 excl = 0;
-        if (tile == 0) {
-            st_release(status, ST_PREFIX | block_total);
-        } else {
-            st_release(status + tile, ST_AGG | block_total);
-            long long p = (long long)tile - 1;
-            u32 spins = 0;
-            while (p >= 0) {
-                u64 w = ld_acquire(status + p);
-                if ((w >> 62) == 0) {
-                    if (++spins > SCAN_SPIN_LIMIT) {
-                        atomicOr(err, DEVERR_SCAN_TIMEOUT);
-                        break;
-                    }
-                    continue;
-                }
-                excl += w & ST_VALUE;
-                if ((w >> 62) == 2) break;
-                p--;
-            }
-            st_release(status + tile, ST_PREFIX | (excl + block_total));
+        __syncwarp();
+        const u64 block_total = s_warp[SCAN_THREADS / 32 - 1];
+        const u64 excl = scan_lookback(status, tile, block_total, err);
+        if (lane == 0) {
+            s_exclusive = excl;
+            if ((u64)(tile + 1) * SCAN_TILE >= n) *total = excl + block_total;
         }
-        s_exclusive = excl;
-        if ((u64)(tile + 1) * SCAN_TILE >= n) *total = excl + block_total;
     }
     __syncthreads();
-    u64 run = s_exclusive + thread_excl;
+    u64 run = s_exclusive + x - local + (warp ? s_warp[warp - 1] : 0);
+    if (vec) {
 #pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-        if (base + k < n) out[base + k] = run;
-        run += v[k];
+        for (int g = 0; g < SCAN_ITEMS; g += 4) {
+            Board o;  // four offsets, one 256-bit store
+            o.bb[0] = run, run += v[g];
+            o.bb[1] = run, run += v[g + 1];
+            o.bb[2] = run, run += v[g + 2];
+            o.bb[3] = run, run += v[g + 3];
+            store_board(reinterpret_cast<Board *>(out + base + g), o);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; k++) {
+            if (base + k < n) out[base + k] = run;
+            run += v[k];
+        }
     }
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan(const u32 *__restrict__ in, u64 n, u64 *__restrict__ out,
+                                                       u64 *__restrict__ status, u32 *__restrict__ ticket,
+                                                       u64 *__restrict__ total, u32 *__restrict__ err)
+{
+    __shared__ u32 s_tile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    scan_tile(in, n, out, status, s_tile, total, err);
 }
 
 // ---------------------------------------------------------------- generate
 // Each thread owns one position of the level; its moves go to
 // [offs[i], offs[i] + counts[i]) of the next level as (parent i, move).
 constexpr int GEN_THREADS = 128;
-constexpr int GEN_CAP = 8192;  // moves staged per CTA (6 B each = 48 KB)
+// Staged moves per thread of a CTA.  A staged move takes 3 bytes of shared
+// memory: the move and the index of the thread (position) that owns it; the
+// copy-out turns that index into the global parent index.
+// Against 6 bytes (move + global parent index) this raised the resident
+// warps from 16 to 36 per SM and cut the generation time 1.64x on B200; 48
+// instead of 64 moves per thread, or a register cap for more warps, gained
+// nothing more.
+constexpr int GEN_MPT = 64;
+constexpr int GEN_CAP = GEN_THREADS * GEN_MPT;  // moves staged per CTA of k_generate_dev
 
 // Both sinks stop at `cap` moves: the level was sized with the exact count,
 // so more moves than that means the count and the generator disagree; the
@@ -180,15 +244,15 @@ constexpr int GEN_CAP = 8192;  // moves staged per CTA (6 B each = 48 KB)
 // written past the allocation.
 struct SmemSink {
     uint16_t *mv;
-    u32 *pi;
-    u32 parent;
+    uint8_t *owner;  // thread index of the position each move belongs to
+    uint8_t me;
     int n, cap;
     bool over;
     __device__ __forceinline__ void put(uint16_t m)
     {
         if (n < cap) {
             mv[n] = m;
-            pi[n] = parent;
+            owner[n] = me;
         } else {
             over = true;
         }
@@ -215,14 +279,15 @@ struct GlobalSink {
 
 template <int C, int GT = GEN_THREADS>
 __global__ void __launch_bounds__(GT) k_generate(const Board *__restrict__ boards,
-                                                 const uint8_t *__restrict__ states,
-                                                 const u64 *__restrict__ offs, const u64 *__restrict__ total,
-                                                 u64 n, uint16_t *__restrict__ out_mv,
-                                                 u32 *__restrict__ out_pi, u32 *__restrict__ err)
+                                             const uint8_t *__restrict__ states,
+                                             const u64 *__restrict__ offs, const u64 *__restrict__ total,
+                                             u64 n, uint16_t *__restrict__ out_mv,
+                                             u32 *__restrict__ out_pi, u32 *__restrict__ err)
 {
-    constexpr int CAP = GT * 64;  // staged moves per CTA (6 B each)
+    static_assert(GT <= 256, "owner indices are one byte");
+    constexpr int CAP = GT * GEN_MPT;  // staged moves per CTA (3 B each)
     __shared__ uint16_t s_mv[CAP];
-    __shared__ u32 s_pi[CAP];
+    __shared__ uint8_t s_own[CAP];
     const u64 first = (u64)blockIdx.x * GT;
     const u64 last = min(first + GT, n);  // exclusive
     const u64 tile_begin = offs[first];
@@ -238,7 +303,8 @@ __global__ void __launch_bounds__(GT) k_generate(const Board *__restrict__ board
         if (mine_end == mine_begin) {
             // no moves allotted: mate, stalemate, a TT hit or a duplicate
         } else if (staged) {
-            SmemSink s{s_mv, s_pi, (u32)i, (int)(mine_begin - tile_begin), (int)(mine_end - tile_begin), false};
+            SmemSink s{s_mv, s_own, (uint8_t)threadIdx.x, (int)(mine_begin - tile_begin),
+                       (int)(mine_end - tile_begin), false};
             gen_moves<C>(b, st, s);
             over = s.over || s.n != s.cap;
         } else {
@@ -253,7 +319,7 @@ __global__ void __launch_bounds__(GT) k_generate(const Board *__restrict__ board
     const int cnt = (int)(tile_end - tile_begin);
     for (int k = threadIdx.x; k < cnt; k += GT) {
         out_mv[tile_begin + k] = s_mv[k];
-        out_pi[tile_begin + k] = s_pi[k];
+        out_pi[tile_begin + k] = (u32)first + s_own[k];
     }
 }
 
@@ -606,71 +672,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_dev(const u32 *__restrict
         if (n == 0 && s_tile == 0 && threadIdx.x == 0) *total = 0;
         return;
     }
-    __shared__ u64 s_warp[SCAN_THREADS / 32];
-    __shared__ u64 s_exclusive;
-    const u32 tile = s_tile;
-    const u64 base = (u64)tile * SCAN_TILE + (u64)threadIdx.x * SCAN_ITEMS;
-    u32 v[SCAN_ITEMS];
-    u64 local = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-        v[k] = (base + k < n) ? in[base + k] : 0u;
-        local += v[k];
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    u64 x = local;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        u64 y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        u64 w = (lane < SCAN_THREADS / 32) ? s_warp[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < SCAN_THREADS / 32; o <<= 1) {
-            u64 y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < SCAN_THREADS / 32) s_warp[lane] = w;
-    }
-    __syncthreads();
-    const u64 block_total = s_warp[SCAN_THREADS / 32 - 1];
-    u64 thread_excl = x - local + (warp ? s_warp[warp - 1] : 0);
-    if (threadIdx.x == 0) {
-        u64 excl = 0;
-        if (tile == 0) {
-            st_release(status, ST_PREFIX | block_total);
-        } else {
-            st_release(status + tile, ST_AGG | block_total);
-            long long p = (long long)tile - 1;
-            u32 spins = 0;
-            while (p >= 0) {
-                u64 w = ld_acquire(status + p);
-                if ((w >> 62) == 0) {
-                    if (++spins > SCAN_SPIN_LIMIT) {
-                        atomicOr(err, DEVERR_SCAN_TIMEOUT);
-                        break;
-                    }
-                    continue;
-                }
-                excl += w & ST_VALUE;
-                if ((w >> 62) == 2) break;
-                p--;
-            }
-            st_release(status + tile, ST_PREFIX | (excl + block_total));
-        }
-        s_exclusive = excl;
-        if ((u64)(tile + 1) * SCAN_TILE >= n) *total = excl + block_total;
-    }
-    __syncthreads();
-    u64 run = s_exclusive + thread_excl;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-        if (base + k < n) out[base + k] = run;
-        run += v[k];
-    }
+    scan_tile(in, n, out, status, s_tile, total, err);
 }
 
 // Generation with device-resident sizes: positions [0, npos) (npos from the
@@ -685,7 +687,7 @@ __global__ void __launch_bounds__(GEN_THREADS) k_generate_dev(const Board *__res
                                                               u32 *__restrict__ err)
 {
     __shared__ uint16_t s_mv[GEN_CAP];
-    __shared__ u32 s_pi[GEN_CAP];
+    __shared__ uint8_t s_own[GEN_CAP];
     const u64 n = dev_size(npos_dev, npos_cap, err);
     const u64 total = *total_dev;
     const u64 first = (u64)blockIdx.x * GEN_THREADS;
@@ -707,7 +709,8 @@ __global__ void __launch_bounds__(GEN_THREADS) k_generate_dev(const Board *__res
         }
         if (mine_end <= mine_begin) {
         } else if (staged) {
-            SmemSink s{s_mv, s_pi, (u32)i, (int)(mine_begin - tile_begin), (int)(mine_end - tile_begin), false};
+            SmemSink s{s_mv, s_own, (uint8_t)threadIdx.x, (int)(mine_begin - tile_begin),
+                       (int)(mine_end - tile_begin), false};
             gen_moves<C>(b, st, s);
             over = s.over || s.n < s.cap;
         } else {
@@ -723,7 +726,7 @@ __global__ void __launch_bounds__(GEN_THREADS) k_generate_dev(const Board *__res
     const int cnt = end > tile_begin ? (int)(end - tile_begin) : 0;
     for (int k = threadIdx.x; k < cnt; k += GEN_THREADS) {
         out_mv[tile_begin + k] = s_mv[k];
-        out_pi[tile_begin + k] = s_pi[k];
+        out_pi[tile_begin + k] = (u32)first + s_own[k];
     }
 }
 

@@ -29,6 +29,26 @@ def test_scan_matches_torch(gpu_engine):
         assert int(d_tot.item()) == int(x.sum()), n
 
 
+def test_scan_unaligned_and_many_tiles(gpu_engine):
+    """Arrays not on a 32-byte boundary take the scalar path; 40 M counts
+    (19,532 tiles) exercise long look-back chains."""
+    import torch
+
+    g = torch.Generator().manual_seed(1)
+    for n, shift in ((2049, 1), (1_000_001, 3), (40_000_000, 0)):
+        x = torch.randint(0, 219, (n,), generator=g, dtype=torch.int64)
+        buf_in = torch.empty(n + shift, dtype=torch.int32, device="cuda")
+        buf_out = torch.empty(n + shift, dtype=torch.int64, device="cuda")
+        d_in, d_out = buf_in[shift:], buf_out[shift:]
+        d_in.copy_(x.to(torch.int32))
+        d_tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+        gpu_engine.dev_scan(d_in.data_ptr(), n, d_out.data_ptr(), d_tot.data_ptr())
+        torch.cuda.synchronize()
+        excl = torch.cumsum(x, 0) - x
+        assert torch.equal(d_out.cpu(), excl), (n, shift)
+        assert int(d_tot.item()) == int(x.sum()), (n, shift)
+
+
 @pytest.mark.parametrize("leaf_kernel", [1, 2])
 def test_gpu_matches_reference_fixtures(gpu_engine, golden, leaf_kernel):
     gpu_engine.set_tuning(leaf_kernel=leaf_kernel)
