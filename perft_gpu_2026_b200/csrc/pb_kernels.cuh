@@ -762,9 +762,12 @@ __global__ void __launch_bounds__(256) k_expand_rooted_dev(const Board *__restri
     }
 }
 
-// Persistent two-ply leaf driven by a device work queue: each warp takes
-// 32-edge chunks from an atomic cursor until the level is exhausted, so
-// uneven subtrees balance across the SMs without a per-edge grid.
+// Persistent two-ply leaf driven by a device work queue: each CTA takes
+// blockDim.x consecutive edges from an atomic cursor until the level is
+// exhausted, so uneven subtrees balance across the SMs without a per-edge
+// grid.  The grab is per CTA, not per warp: the CTA's warps then work on
+// sibling edges whose attack-table lines they share in L1 (per-warp grabs of
+// 32, 64 or 128 edges measured 2.6-6 % slower on B200).
 template <int C, bool STRICT>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_rooted_queue(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
@@ -778,12 +781,14 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     const u64 npar = min(*npar_dev, npar_cap);
     const int lane = threadIdx.x & 31;
     u32 counted = 0;
+    __shared__ unsigned long long s_base;
     for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(cursor, 32ULL);
-        base = __shfl_sync(0xffffffffu, base, 0);
+        if (threadIdx.x == 0) s_base = atomicAdd(cursor, (unsigned long long)blockDim.x);
+        __syncthreads();
+        const unsigned long long base = s_base;
+        __syncthreads();
         if (base >= n) break;
-        const u64 i = base + lane;
+        const u64 i = base + threadIdx.x;
         u32 total = 0, root = 0;
         bool valid = i < n && pidx[i] < npar;
         if (valid) {
