@@ -152,12 +152,14 @@ typedef struct {
 /* Launch parameters of the GPU path (no reference counterpart: the
  * reference fixes them at compile time, switches.h:8-24, perft_kernels.cu:74).
  * Zero fields keep the current value.  leaf_kernel: 1 = one edge per thread,
- * 2 = cooperative (grandchildren spread over the CTA);
+ * 2 = cooperative (grandchildren spread over the CTA), 3 = in-check children
+ * deferred to a second pass, 4 = one edge per thread with the CTA's children
+ * ranked by move count first (default);
  * leaf_blocks_per_sm: persistent grid of the cooperative leaf. */
 typedef struct {
     int leaf_kernel;
     int leaf_blocks_per_sm;
-    int leaf_threads;   /* CTA size of the one-edge-per-thread leaf: 128, 256 (default) or 512 */
+    int leaf_threads;   /* CTA size of leaf kernels 1, 3 and 4: 128, 256 (default) or 512 (not 3) */
     int gen_threads;    /* CTA size of the staged generator: 64 or 128 (default); stages 64 moves per thread */
     int leaf_fuse;      /* plies fused in the leaf kernel: 2 (default) or 1 (one more BFS level) */
     int tt_replace;     /* device TT replacement: 1 = always overwrite (default, tt.h:60-70),

@@ -1,10 +1,11 @@
 """Autotuner for the GPU path's launch parameters.
 
-Candidates: leaf kernel (one edge per thread / cooperative), the leaf's CTA
-size (128/256/512), the staged generator's CTA size and tile (64 or 128
+Candidates: leaf kernel (one edge per thread / cooperative / one edge per
+thread with the CTA's children ranked by move count), the leaf's CTA size
+(128/256/512), the staged generator's CTA size and tile (64 or 128
 threads, 64 moves staged per thread) and the leaf fuse depth (two plies fused
-in the leaf, or one with an extra BFS level).  Each candidate runs a sample
-perft on the GPU (device time from the engine's CUDA events, median of 3);
+in the leaf, or one with an extra BFS level).  Each candidate runs perft 7
+of the bench position on the GPU (device time from the engine's CUDA events, median of 3);
 the fastest is cached per GPU model and driver in
 $XDG_CACHE_HOME/perft_b200/tuning.json (default ~/.cache/perft_b200) and
 applied to the engine.
@@ -13,6 +14,7 @@ applied to the engine.
 """
 from __future__ import annotations
 
+import hashlib
 import itertools
 import json
 import os
@@ -40,6 +42,8 @@ def candidates() -> List[Dict[str, int]]:
     for lt, gt, fuse in itertools.product((128, 256, 512), (64, 128), (2, 1)):
         out.append({"leaf_kernel": 1, "leaf_threads": lt, "gen_threads": gt, "leaf_fuse": fuse})
     out.append({"leaf_kernel": 2, "leaf_threads": 256, "gen_threads": 128, "leaf_fuse": 2})
+    for gt in (64, 128):
+        out.append({"leaf_kernel": 4, "leaf_threads": 256, "gen_threads": gt, "leaf_fuse": 2})
     return out
 
 
@@ -54,7 +58,7 @@ def measure(eng: pg.Engine, cfg: Dict[str, int], pos: pg.Pos, depth: int, reps: 
     return statistics.median(ms)
 
 
-def tune(eng: pg.Engine, pos: Optional[pg.Pos] = None, depth: int = 6, verbose: bool = False) -> Dict:
+def tune(eng: pg.Engine, pos: Optional[pg.Pos] = None, depth: int = 7, verbose: bool = False) -> Dict:
     pos = pos or pg.config_position(4, 1)
     results = []
     ref = None
@@ -80,7 +84,10 @@ def tune(eng: pg.Engine, pos: Optional[pg.Pos] = None, depth: int = 6, verbose: 
 
 
 def load_or_tune(eng: pg.Engine, device: int = 0, retune: bool = False) -> Dict:
-    key = gpu_key(device)
+    # the candidate list is part of the key: a cache made with other
+    # candidates is not reused
+    tag = hashlib.sha1(json.dumps(candidates(), sort_keys=True).encode()).hexdigest()[:12]
+    key = f"{gpu_key(device)}|{tag}"
     cache = {}
     if os.path.exists(CACHE):
         try:

@@ -70,7 +70,7 @@ struct pb_ctx {
     u64 *h_pinned = nullptr;  // pinned host words for readbacks
     int launch_depth = 0;
     bool timing = false;
-    pb_tuning tuning{1, 0, 256, 128, 2, 1, {0, 0}};
+    pb_tuning tuning{4, 0, 256, 128, 2, 1, {0, 0}};
     int num_sms = 0;
     uint16_t *spill = nullptr;  // cooperative-leaf spill area (device)
     size_t spill_blocks = 0;
@@ -190,6 +190,15 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
         switch (ctx->tuning.leaf_threads) {
         case 128: k_leaf2_defer<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         default: k_leaf2_defer<C, S, 256><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        }
+        PB_CUDA(cudaGetLastError());
+        return PB_OK;
+    }
+    if (ctx->tuning.leaf_kernel == 4) {
+        switch (ctx->tuning.leaf_threads) {
+        case 128: k_leaf2_sorted<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        case 512: k_leaf2_sorted<C, S, 512><<<grid_for(n, 512), 512, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        default: k_leaf2_sorted<C, S, 256><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         }
         PB_CUDA(cudaGetLastError());
         return PB_OK;
@@ -1470,7 +1479,7 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
 {
     if (!ctx || !t) return PB_ERR_ARG;
     if (t->leaf_kernel) {
-        if (t->leaf_kernel < 1 || t->leaf_kernel > 3) return PB_ERR_ARG;
+        if (t->leaf_kernel < 1 || t->leaf_kernel > 4) return PB_ERR_ARG;
         ctx->tuning.leaf_kernel = t->leaf_kernel;
     }
     if (t->leaf_blocks_per_sm) {

@@ -49,8 +49,9 @@ def test_scan_unaligned_and_many_tiles(gpu_engine):
         assert int(d_tot.item()) == int(x.sum()), (n, shift)
 
 
-@pytest.mark.parametrize("leaf_kernel", [1, 2])
+@pytest.mark.parametrize("leaf_kernel", [1, 2, 4])
 def test_gpu_matches_reference_fixtures(gpu_engine, golden, leaf_kernel):
+    prev = gpu_engine.get_tuning().leaf_kernel
     gpu_engine.set_tuning(leaf_kernel=leaf_kernel)
     bad = []
     for case in golden:
@@ -59,7 +60,7 @@ def test_gpu_matches_reference_fixtures(gpu_engine, golden, leaf_kernel):
             got = gpu_engine.perft_position(p, d)
             if got != want:
                 bad.append((case["name"], d, got, want))
-    gpu_engine.set_tuning(leaf_kernel=2)
+    gpu_engine.set_tuning(leaf_kernel=prev)
     assert not bad, bad
 
 
@@ -88,13 +89,14 @@ def test_strict_mode_counts_merged_moves(oracle):
     comp.close()
 
 
-@pytest.mark.parametrize("leaf_kernel", [1, 2])
+@pytest.mark.parametrize("leaf_kernel", [1, 2, 4])
 def test_readme_known_totals(gpu_engine, leaf_kernel):
     # README.md:51-52 and :92 (RTX PRO 6000 / GB10 tables)
+    prev = gpu_engine.get_tuning().leaf_kernel
     gpu_engine.set_tuning(leaf_kernel=leaf_kernel)
     assert gpu_engine.perft_position(pg.parse_fen(START), 8) == 84_998_978_956
     assert gpu_engine.perft_position(pg.parse_fen(KIWIPETE), 7) == 374_190_009_323
-    gpu_engine.set_tuning(leaf_kernel=2)
+    gpu_engine.set_tuning(leaf_kernel=prev)
 
 
 def test_readme_startpos_perft9(gpu_engine):
