@@ -40,7 +40,10 @@ sys.path.insert(0, ROOT)
 WORKLOAD = {"workload": "single-position perft", "position": "4 random plies from the initial array, splitmix64 seed 1",
             "depth": 7, "tt": False}
 METRIC = "leaf nodes/s"
-PROFILE_INST_PER_POSITION = None  # filled from profiles/ once ncu has measured it
+
+
+# leaf kernel launched for each pb_tuning.leaf_kernel value
+LEAF_KERNELS = {1: "k_leaf2", 2: "k_leaf2_coop", 3: "k_leaf2_defer", 4: "k_leaf2_sorted"}
 
 
 def _load_profile_constants():
@@ -348,7 +351,8 @@ def main():
         nodes = int(c.item())
     if rank == 0:
         peaks, peak_kind = _peaks()
-        consts = _load_profile_constants()
+        kernel = LEAF_KERNELS.get(eng.get_tuning().leaf_kernel, "k_leaf2")
+        consts = _load_profile_constants().get(kernel, {})
         leaf_pos = results[0][3]
         kernels = results[0][4]
         sm_mhz = peaks.get("sm_max_mhz", 1965.0)
@@ -357,7 +361,7 @@ def main():
         dram_per_pos = consts.get("dram_bytes_per_position")
         roofline = {"bound": "int_issue", "unit": "Gwarp-inst/s", "peak": issue_peak,
                     "peak_source": f"148 SMs x 4 warp-inst issue/clk x sm_max_mhz ({peak_kind})",
-                    "kernel": "k_leaf2", "leaf_ms": my_leaf_ms, "positions_per_launch": leaf_pos,
+                    "kernel": kernel, "leaf_ms": my_leaf_ms, "positions_per_launch": leaf_pos,
                     "positions_per_s": leaf_pos / (my_leaf_ms / 1e3) if my_leaf_ms > 0 else None,
                     "achieved": None, "frac": None,
                     "traffic": dram_per_pos * leaf_pos if dram_per_pos else None,
