@@ -39,6 +39,7 @@ struct GraphPlan {
     u64 n = 0;
     int depth = 0;
     bool strict = false;
+    bool sort = false;  // leaf ranks each CTA's children by move count
     std::vector<u64> caps;
     cudaGraphExec_t exec = nullptr;
     // device buffers inside the arena (fixed for the captured graph)
@@ -47,9 +48,9 @@ struct GraphPlan {
     u32 *r0 = nullptr;
     unsigned long long *rc = nullptr;
     u64 *sizes = nullptr;
-    bool same(u64 n_, int d_, bool s_, const std::vector<u64> &c_) const
+    bool same(u64 n_, int d_, bool s_, bool sort_, const std::vector<u64> &c_) const
     {
-        return exec && n == n_ && depth == d_ && strict == s_ && caps == c_;
+        return exec && n == n_ && depth == d_ && strict == s_ && sort == sort_ && caps == c_;
     }
 };
 
@@ -789,13 +790,28 @@ int bfs_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth,
             }
         } else {
             unsigned g = grid_for(ne, PB_LEAF_THREADS);
+            const bool sort = ctx->tuning.leaf_kernel == 4;
+#define PB_ROOTED_LEAF(CC, SS)                                                                                   \
+    if (sort)                                                                                                    \
+        k_leaf2_rooted<CC, SS, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, \
+                                                                   ctx->d_counter);                              \
+    else                                                                                                         \
+        k_leaf2_rooted<CC, SS, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, \
+                                                                    ctx->d_counter);
             if (c == WHITE) {
-                if (strict) k_leaf2_rooted<WHITE, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, ctx->d_counter);
-                else k_leaf2_rooted<WHITE, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, ctx->d_counter);
+                if (strict) {
+                    PB_ROOTED_LEAF(WHITE, true)
+                } else {
+                    PB_ROOTED_LEAF(WHITE, false)
+                }
             } else {
-                if (strict) k_leaf2_rooted<BLACK, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, ctx->d_counter);
-                else k_leaf2_rooted<BLACK, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, ctx->d_counter);
+                if (strict) {
+                    PB_ROOTED_LEAF(BLACK, true)
+                } else {
+                    PB_ROOTED_LEAF(BLACK, false)
+                }
             }
+#undef PB_ROOTED_LEAF
         }
         PB_CUDA(cudaGetLastError());
         stats.kernels += 1;
@@ -858,17 +874,28 @@ struct GraphLevel {
     u64 tiles;
 };
 
-template <int C, bool S>
-void launch_leaf_queue(cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r, const u32 *pi,
-                       const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev, u64 npar_cap,
-                       unsigned long long *cursor, unsigned long long *rc, unsigned long long *counter, u32 *err)
+template <int C, bool S, bool SORT>
+void launch_leaf_queue_t(cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r, const u32 *pi,
+                         const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev, u64 npar_cap,
+                         unsigned long long *cursor, unsigned long long *rc, unsigned long long *counter, u32 *err)
 {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf2_rooted_queue<C, S>, PB_LEAF_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf2_rooted_queue<C, S, SORT>, PB_LEAF_THREADS, 0);
     if (per_sm <= 0) per_sm = 1;
     unsigned grid = (unsigned)std::min<u64>((u64)sms * per_sm, (cap + PB_LEAF_THREADS - 1) / PB_LEAF_THREADS + 1);
-    k_leaf2_rooted_queue<C, S><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap,
-                                                                cursor, rc, counter, err);
+    k_leaf2_rooted_queue<C, S, SORT><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev,
+                                                                      npar_cap, cursor, rc, counter, err);
+}
+template <int C, bool S>
+void launch_leaf_queue(bool sort, cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r,
+                       const u32 *pi, const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev,
+                       u64 npar_cap, unsigned long long *cursor, unsigned long long *rc, unsigned long long *counter,
+                       u32 *err)
+{
+    if (sort)
+        launch_leaf_queue_t<C, S, true>(s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc, counter, err);
+    else
+        launch_leaf_queue_t<C, S, false>(s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc, counter, err);
 }
 
 // Builds (captures) the graph for a planned batch shape.
@@ -978,17 +1005,17 @@ int capture_batch_graph(pb_ctx *ctx, GraphPlan &g)
                                                                 npar_cap, g.rc, ctx->d_err);
     } else if (c == WHITE) {
         if (g.strict)
-            launch_leaf_queue<WHITE, true>(s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
+            launch_leaf_queue<WHITE, true>(g.sort, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
                                            npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
         else
-            launch_leaf_queue<WHITE, false>(s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
+            launch_leaf_queue<WHITE, false>(g.sort, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
                                             npar, npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
     } else {
         if (g.strict)
-            launch_leaf_queue<BLACK, true>(s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
+            launch_leaf_queue<BLACK, true>(g.sort, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
                                            npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
         else
-            launch_leaf_queue<BLACK, false>(s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
+            launch_leaf_queue<BLACK, false>(g.sort, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
                                             npar, npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -1008,10 +1035,12 @@ int run_planned_batch(pb_ctx *ctx, GraphPlan &g, const Board *rb, const uint8_t 
 {
     *overflow = false;
     const bool strict = ctx->opts.strict != 0;
-    if (!g.same(n, depth, strict, caps)) {
+    const bool sort = ctx->tuning.leaf_kernel == 4;
+    if (!g.same(n, depth, strict, sort, caps)) {
         g.n = n;
         g.depth = depth;
         g.strict = strict;
+        g.sort = sort;
         g.caps = caps;
         int rc = capture_batch_graph(ctx, g);
         if (rc != PB_OK) {

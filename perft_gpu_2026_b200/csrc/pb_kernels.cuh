@@ -402,34 +402,18 @@ namespace pb {
 // B200 against k_leaf2: +2.5 % on the bench position, +1.6 % on Kiwipete with
 // 256-thread CTAs; 128 or 512 threads, or a pseudo-legal count as the key,
 // balance worse.
-template <int C, bool STRICT, int T>
-__global__ void __launch_bounds__(T, 1024 / T) k_leaf2_sorted(const Board *__restrict__ pboards,
-                                                              const uint8_t *__restrict__ pstates,
-                                                              const u32 *__restrict__ pidx,
-                                                              const uint16_t *__restrict__ moves, u64 n, u64 nparents,
-                                                              unsigned long long *__restrict__ counter)
+// Rank of this thread's key (< 256) among the T keys of its CTA, ascending;
+// equal keys get distinct ranks in arbitrary order.  A shared-memory
+// histogram and its exclusive prefix; every thread of the CTA must call it.
+template <int T> __device__ __forceinline__ u32 cta_rank_u8(u32 key)
 {
-    __shared__ Board s_b[T];
-    __shared__ uint8_t s_st[T];
-    __shared__ uint8_t s_key[T];  // 0 = no child, else 1 + its move count
-    __shared__ u32 s_hist[256];   // histogram of the keys, then exclusive prefix
+    __shared__ u32 s_hist[256];
     __shared__ u32 s_wsum[T / 32];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int k = tid; k < 256; k += T) s_hist[k] = 0;
     __syncthreads();
-    const u64 i = (u64)blockIdx.x * T + tid;
-    Board b{};
-    u32 st = 0, key = 0;
-    if (i < n && pidx[i] < nparents) {
-        u32 p = pidx[i];
-        b = load_board(pboards + p);
-        st = pstates[p];
-        make_move<C>(b, st, moves[i]);
-        key = 1 + min(count_moves<1 - C, true>(b, st), 254u);
-    }
-    const u32 slot = atomicAdd(&s_hist[key], 1u);  // order among equal keys
+    const u32 slot = atomicAdd(&s_hist[key], 1u);
     __syncthreads();
-    // exclusive prefix of the 256-bin histogram
     constexpr int PER = T >= 256 ? 1 : 256 / T;
     u32 h[PER], local = 0;
 #pragma unroll
@@ -437,7 +421,6 @@ __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_sorted(const Board *__res
         h[k] = (tid * PER + k < 256) ? s_hist[tid * PER + k] : 0u;
         local += h[k];
     }
-    const int lane = tid & 31, warp = tid >> 5;
     u32 x = local;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -455,6 +438,32 @@ __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_sorted(const Board *__res
     }
     __syncthreads();
     const u32 rank = s_hist[key] + slot;
+    __syncthreads();  // s_hist is free again for the next call
+    return rank;
+}
+
+template <int C, bool STRICT, int T>
+__global__ void __launch_bounds__(T, 1024 / T) k_leaf2_sorted(const Board *__restrict__ pboards,
+                                                              const uint8_t *__restrict__ pstates,
+                                                              const u32 *__restrict__ pidx,
+                                                              const uint16_t *__restrict__ moves, u64 n, u64 nparents,
+                                                              unsigned long long *__restrict__ counter)
+{
+    __shared__ Board s_b[T];
+    __shared__ uint8_t s_st[T];
+    __shared__ uint8_t s_key[T];  // 0 = no child, else 1 + its move count
+    const int tid = threadIdx.x;
+    const u64 i = (u64)blockIdx.x * T + tid;
+    Board b{};
+    u32 st = 0, key = 0;
+    if (i < n && pidx[i] < nparents) {
+        u32 p = pidx[i];
+        b = load_board(pboards + p);
+        st = pstates[p];
+        make_move<C>(b, st, moves[i]);
+        key = 1 + min(count_moves<1 - C, true>(b, st), 254u);
+    }
+    const u32 rank = cta_rank_u8<T>(key);
     s_b[rank] = b;
     s_st[rank] = (uint8_t)st;
     s_key[rank] = (uint8_t)key;
@@ -476,7 +485,7 @@ __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_sorted(const Board *__res
     }
     total = __reduce_add_sync(0xffffffffu, total);
     counted = __reduce_add_sync(0xffffffffu, counted);
-    if (lane == 0 && counted) {
+    if ((tid & 31) == 0 && counted) {
         atomicAdd(counter, (unsigned long long)total);
         atomicAdd(counter + 1, (unsigned long long)counted);
     }
@@ -671,8 +680,35 @@ __device__ __forceinline__ void add_by_key(unsigned long long *out, u32 key, u32
     if ((int)(threadIdx.x & 31) == __ffs(peers) - 1 && total) atomicAdd(out + key, (unsigned long long)total);
 }
 
-// Two-ply leaf over edges, counts credited to each edge's root.
-template <int C, bool STRICT>
+// Children of a CTA (one per thread) handed to threads in order of their
+// move counts, as in k_leaf2_sorted, carrying their root index along.  On
+// return thread t holds the child of rank t; `valid` says whether it has one.
+template <int C, int T>
+__device__ __forceinline__ void rank_children(Board &b, u32 &st, u32 &root, bool &valid)
+{
+    __shared__ Board s_b[T];
+    __shared__ u32 s_root[T];
+    __shared__ uint8_t s_st[T];
+    __shared__ uint8_t s_key[T];
+    const u32 key = valid ? 1 + min(count_moves<1 - C, true>(b, st), 254u) : 0u;
+    const u32 rank = cta_rank_u8<T>(key);
+    s_b[rank] = b;
+    s_root[rank] = root;
+    s_st[rank] = (uint8_t)st;
+    s_key[rank] = (uint8_t)key;
+    __syncthreads();
+    const int tid = threadIdx.x;
+    b = s_b[tid];
+    root = s_root[tid];
+    st = s_st[tid];
+    valid = s_key[tid] != 0;
+    __syncthreads();  // the exchange arrays are free again
+}
+
+// Two-ply leaf over edges, counts credited to each edge's root.  With SORT
+// the CTA's children are ranked by move count first (blockDim.x must be
+// PB_LEAF_THREADS).
+template <int C, bool STRICT, bool SORT = false>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_rooted(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                    const u32 *__restrict__ proot, const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
@@ -682,12 +718,17 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     u32 total = 0, counted = 0, root = 0;
     bool valid = i < n && pidx[i] < nparents;
+    Board b{};
+    u32 st = 0;
     if (valid) {
         u32 p = pidx[i];
         root = proot[p];
-        Board b = load_board(pboards + p);
-        u32 st = pstates[p];
+        b = load_board(pboards + p);
+        st = pstates[p];
         make_move<C>(b, st, moves[i]);
+    }
+    if (SORT) rank_children<C, PB_LEAF_THREADS>(b, st, root, valid);
+    if (valid) {
         uint16_t mv[MAX_MOVES];
         ArraySink sink{mv, 0};
         gen_moves<1 - C>(b, st, sink);
@@ -861,7 +902,7 @@ __global__ void __launch_bounds__(256) k_expand_rooted_dev(const Board *__restri
 // grid.  The grab is per CTA, not per warp: the CTA's warps then work on
 // sibling edges whose attack-table lines they share in L1 (per-warp grabs of
 // 32, 64 or 128 edges measured 2.6-6 % slower on B200).
-template <int C, bool STRICT>
+template <int C, bool STRICT, bool SORT = false>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_rooted_queue(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                          const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
@@ -884,12 +925,17 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
         const u64 i = base + threadIdx.x;
         u32 total = 0, root = 0;
         bool valid = i < n && pidx[i] < npar;
+        Board b{};
+        u32 st = 0;
         if (valid) {
             u32 p = pidx[i];
             root = proot[p];
-            Board b = load_board(pboards + p);
-            u32 st = pstates[p];
+            b = load_board(pboards + p);
+            st = pstates[p];
             make_move<C>(b, st, moves[i]);
+        }
+        if (SORT) rank_children<C, PB_LEAF_THREADS>(b, st, root, valid);
+        if (valid) {
             uint16_t mv[MAX_MOVES];
             ArraySink sink{mv, 0};
             gen_moves<1 - C>(b, st, sink);
