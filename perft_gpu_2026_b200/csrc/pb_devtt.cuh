@@ -253,8 +253,12 @@ __global__ void k_dedup_resolve(const Hash128 *__restrict__ h, uint8_t *__restri
     }
 }
 
-// Leaf with the depth-2 table: perft 2 of each edge's child, per edge.
-template <int C, bool STRICT>
+// Leaf with the depth-2 table: perft 2 of each edge's child, per edge.  With
+// SORT (blockDim.x must be PB_LEAF_THREADS) table hits are answered first and
+// the CTA's misses are ranked by move count and handed to threads in that
+// order, so the misses fill whole warps (all-hit warps then have no work) and
+// each warp's misses have similar loop lengths.
+template <int C, bool STRICT, bool SORT = false>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_tt(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                const Hash128 *__restrict__ phash, const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
@@ -262,30 +266,56 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
 {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     u32 total = 0, counted = 0;
+    bool miss = false;
+    Board b{};
+    u32 st = 0;
+    Hash128 h{};
     if (i < n && pidx[i] < nparents) {
         u32 p = pidx[i];
-        Board b = load_board(pboards + p);
-        u32 st = pstates[p];
+        b = load_board(pboards + p);
+        st = pstates[p];
         Board before = b;
         uint16_t mv0 = moves[i];
         make_move<C>(b, st, mv0);
-        Hash128 h = hash_move(phash[p], before, pstates[p], st, C, mv0);
+        h = hash_move(phash[p], before, pstates[p], st, C, mv0);
         u64 hit;
-        if (tt_probe(tt, h, &hit)) {
-            total = (u32)hit;
-        } else {
-            uint16_t mv[MAX_MOVES];
-            ArraySink sink{mv, 0};
-            gen_moves<1 - C>(b, st, sink);
-            for (int k = 0; k < sink.n; k++) {
-                Board g = b;
-                u32 gs = st;
-                make_move<1 - C>(g, gs, mv[k]);
-                total += count_moves<C, STRICT>(g, gs);
-            }
-            counted = sink.n;
-            tt_store(tt, h, total);
+        if (tt_probe(tt, h, &hit))
+            out[i] = (u32)hit;
+        else
+            miss = true;
+    }
+    if (SORT) {
+        __shared__ Board s_b[PB_LEAF_THREADS];
+        __shared__ Hash128 s_h[PB_LEAF_THREADS];
+        __shared__ u32 s_i[PB_LEAF_THREADS];
+        __shared__ uint8_t s_st[PB_LEAF_THREADS];
+        __shared__ uint8_t s_key[PB_LEAF_THREADS];
+        const u32 key = miss ? 1 + min(count_moves<1 - C, true>(b, st), 254u) : 0u;
+        const u32 rank = cta_rank_u8<PB_LEAF_THREADS>(key);
+        s_b[rank] = b;
+        s_h[rank] = h;
+        s_i[rank] = (u32)(i - (u64)blockIdx.x * blockDim.x);
+        s_st[rank] = (uint8_t)st;
+        s_key[rank] = (uint8_t)key;
+        __syncthreads();
+        b = s_b[threadIdx.x];
+        h = s_h[threadIdx.x];
+        i = (u64)blockIdx.x * blockDim.x + s_i[threadIdx.x];
+        st = s_st[threadIdx.x];
+        miss = s_key[threadIdx.x] != 0;
+    }
+    if (miss) {
+        uint16_t mv[MAX_MOVES];
+        ArraySink sink{mv, 0};
+        gen_moves<1 - C>(b, st, sink);
+        for (int k = 0; k < sink.n; k++) {
+            Board g = b;
+            u32 gs = st;
+            make_move<1 - C>(g, gs, mv[k]);
+            total += count_moves<C, STRICT>(g, gs);
         }
+        counted = sink.n;
+        tt_store(tt, h, total);
         out[i] = total;
     }
     counted = __reduce_add_sync(0xffffffffu, counted);

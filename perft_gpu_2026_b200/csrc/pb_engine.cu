@@ -538,17 +538,28 @@ int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int dep
     if (n > 0) {
         TTView tv = ctx->dtt.at(2);
         unsigned g = grid_for(n, PB_LEAF_THREADS);
+        const bool sort = ctx->tuning.leaf_kernel == 4;
+#define PB_TT_LEAF(CC, SS)                                                                                     \
+    if (sort)                                                                                                  \
+        k_leaf2_tt<CC, SS, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,     \
+                                                               leafcnt, ctx->d_counter);                      \
+    else                                                                                                       \
+        k_leaf2_tt<CC, SS, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,    \
+                                                                leafcnt, ctx->d_counter);
         if (c == WHITE) {
-            if (strict)
-                k_leaf2_tt<WHITE, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, leafcnt, ctx->d_counter);
-            else
-                k_leaf2_tt<WHITE, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, leafcnt, ctx->d_counter);
+            if (strict) {
+                PB_TT_LEAF(WHITE, true)
+            } else {
+                PB_TT_LEAF(WHITE, false)
+            }
         } else {
-            if (strict)
-                k_leaf2_tt<BLACK, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, leafcnt, ctx->d_counter);
-            else
-                k_leaf2_tt<BLACK, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv, leafcnt, ctx->d_counter);
+            if (strict) {
+                PB_TT_LEAF(BLACK, true)
+            } else {
+                PB_TT_LEAF(BLACK, false)
+            }
         }
+#undef PB_TT_LEAF
         PB_CUDA(cudaGetLastError());
         stats.kernels += 1;
     }
