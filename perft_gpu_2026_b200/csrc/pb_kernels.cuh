@@ -402,17 +402,21 @@ namespace pb {
 // B200 against k_leaf2: +2.5 % on the bench position, +1.6 % on Kiwipete with
 // 256-thread CTAs; 128 or 512 threads, or a pseudo-legal count as the key,
 // balance worse.
-// Rank of this thread's key (< 256) among the T keys of its CTA, ascending;
-// equal keys get distinct ranks in arbitrary order.  A shared-memory
-// histogram and its exclusive prefix; every thread of the CTA must call it.
-template <int T> __device__ __forceinline__ u32 cta_rank_u8(u32 key)
+// Ranks of this thread's K keys (each < 256) among the K * T keys of its CTA,
+// ascending; equal keys get distinct ranks in arbitrary order.  `below1` =
+// how many keys are 0.  A shared-memory histogram and its exclusive prefix;
+// every thread of the CTA must call it.
+template <int T, int K>
+__device__ __forceinline__ void cta_rank_u8(const u32 (&key)[K], u32 (&rank)[K], u32 *below1 = nullptr)
 {
     __shared__ u32 s_hist[256];
     __shared__ u32 s_wsum[T / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int k = tid; k < 256; k += T) s_hist[k] = 0;
     __syncthreads();
-    const u32 slot = atomicAdd(&s_hist[key], 1u);
+    u32 slot[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) slot[k] = atomicAdd(&s_hist[key[k]], 1u);
     __syncthreads();
     constexpr int PER = T >= 256 ? 1 : 256 / T;
     u32 h[PER], local = 0;
@@ -437,9 +441,16 @@ template <int T> __device__ __forceinline__ u32 cta_rank_u8(u32 key)
         base += h[k];
     }
     __syncthreads();
-    const u32 rank = s_hist[key] + slot;
+#pragma unroll
+    for (int k = 0; k < K; k++) rank[k] = s_hist[key[k]] + slot[k];
+    if (below1) *below1 = s_hist[1];
     __syncthreads();  // s_hist is free again for the next call
-    return rank;
+}
+template <int T> __device__ __forceinline__ u32 cta_rank_u8(u32 key)
+{
+    u32 k[1] = {key}, r[1];
+    cta_rank_u8<T, 1>(k, r);
+    return r[0];
 }
 
 template <int C, bool STRICT, int T>
