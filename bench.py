@@ -21,8 +21,8 @@ Printed JSON line (rank 0):
   positions  (one GPU) positions/s on 4096 uneven roots at perft 5: plain
            per-root calls, count-then-allocate batch, learned planner
 With --gpus N > 1 (torchrun, one process per GPU) the depth-2 subtrees of the
-root are split over the ranks (strong scaling: total work fixed); the only
-exchange is one all-reduce of the per-rank counts.
+root are bin-packed over the ranks by their perft(2) (strong scaling: total
+work fixed); the only exchange is one all-reduce of the per-rank counts.
 """
 from __future__ import annotations
 
@@ -290,11 +290,13 @@ def main():
             tuning = autotune.load_or_tune(eng, local)["best"]
     eng.set_timing(True)
 
-    # shard: depth-2 subtrees round-robin over ranks (one rank: the whole root)
+    # shard: depth-2 subtrees bin-packed over ranks by their perft(2), an exact
+    # size estimate every rank computes identically (one rank: the whole root)
     from perft_gpu_2026_b200 import dist as pdist
 
     if world > 1:
-        mine = pdist.shard(pdist.subtrees(root, 2), world, rank)
+        subs = pdist.subtrees(root, 2)
+        mine = pdist.shard_balanced(subs, eng.perft_batch(subs, [2] * len(subs)), world, rank)
         sub_depth = depth - 2
     else:
         mine = [root]

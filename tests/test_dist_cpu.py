@@ -19,7 +19,7 @@ def _free_port():
     return port
 
 
-def _worker(rank, world, port, fen, depth, q):
+def _worker(rank, world, port, fen, depth, balanced, q):
     import datetime
 
     import torch.distributed as dist
@@ -33,19 +33,21 @@ def _worker(rank, world, port, fen, depth, q):
     def count(positions, d):
         return sum(eng.perft_cpu(p, d) for p in positions)
 
-    part = pdist.perft_sharded(root, depth, count, world, rank)
+    weight = (lambda subs: [eng.perft_cpu(p, 2) for p in subs]) if balanced else None
+    part = pdist.perft_sharded(root, depth, count, world, rank, weight=weight)
     total = pdist.all_reduce_count(part)
     q.put((rank, part, total))
     dist.barrier()
     dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("balanced", [False, True])
 @pytest.mark.parametrize("fen,depth", [(pg.START_FEN, 4), ("r3k2r/p1ppqpb1/bn2pnp1/3PN3/1p2P3/2N2Q1p/PPPBBPPP/R3K2R w KQkq -", 3)])
-def test_two_rank_gloo_perft(fen, depth):
+def test_two_rank_gloo_perft(fen, depth, balanced):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, fen, depth, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, fen, depth, balanced, q)) for r in range(2)]
     for p in procs:
         p.start()
     res = [q.get(timeout=120) for _ in procs]
@@ -66,3 +68,28 @@ def test_shard_covers_every_subtree_once():
     assert sum(len(p) for p in parts) == 400
     keys = sorted(s.key() for p in parts for s in p)
     assert keys == sorted(s.key() for s in subs)
+
+
+def test_balanced_assignment_covers_every_item_once_and_balances():
+    w = [float(x) for x in (97, 3, 50, 50, 12, 88, 7, 41, 41, 1, 66, 30)]
+    for world in (1, 2, 3, 4):
+        owner = pdist.balanced_assignment(w, world)
+        assert len(owner) == len(w) and set(owner) <= set(range(world))
+        parts = [pdist.shard_balanced(list(range(len(w))), w, world, r) for r in range(world)]
+        assert sorted(i for p in parts for i in p) == list(range(len(w)))
+        loads = [sum(w[i] for i in p) for p in parts]
+        # greedy LPT: no rank exceeds the mean by more than the largest item
+        assert max(loads) <= sum(w) / world + max(w)
+        assert owner == pdist.balanced_assignment(list(w), world)  # deterministic
+
+
+def test_balanced_beats_round_robin_on_bench_subtrees():
+    root = pg.config_position(4, 1)
+    subs = pdist.subtrees(root, 2)
+    eng = pg.Engine(device=-1)
+    w = [eng.perft_cpu(p, 2) for p in subs]
+    rr = [sum(w[i] for i in range(r, len(w), 4)) for r in range(4)]
+    owner = pdist.balanced_assignment(w, 4)
+    bal = [sum(x for x, o in zip(w, owner) if o == r) for r in range(4)]
+    assert max(bal) <= max(rr)
+    assert max(bal) - min(bal) <= max(w)
