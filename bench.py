@@ -82,6 +82,11 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            # nvidia-smi takes a moment to start: wait (at most 3 s) for its
+            # first sample so the whole timed region is covered
+            t0 = time.time()
+            while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
@@ -220,8 +225,10 @@ def run_reference_arm(args):
     root = pg.config_position(4, 1)
     vals = []
     last = None
+    # each step is a bounded sample; the whole run stays near two minutes
+    per_step = max(1.0, min(8.0, 120.0 / (args.warmup + args.steps)))
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_sample(pg, root, WORKLOAD["depth"], max_seconds=8.0)
+        r = cpu_reference_sample(pg, root, WORKLOAD["depth"], max_seconds=per_step)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/perft_gpu_ref not built"}))
             return 0
@@ -243,7 +250,7 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--depth", type=int, default=WORKLOAD["depth"])
