@@ -228,3 +228,19 @@ def test_deferred_evasion_leaf(golden, threads):
             assert eng.perft_position(p, d) == want, (case["name"], d)
     assert eng.perft_position(pg.parse_fen(KIWIPETE), 6) == 8031647685
     eng.close()
+
+
+MATED = "rnb1kbnr/pppp1ppp/8/4p3/6Pq/5P2/PPPPP2P/RNBQKBNR w KQkq - 1 3"  # side to move is checkmated
+STALEMATE = "7k/5Q2/6K1/8/8/8/8/8 b - - 0 1"  # side to move has no move, not in check
+
+
+def test_edge_depths_and_terminal_positions(gpu_engine, oracle):
+    """perft(0) = 1, terminal roots count 0 at every depth >= 1, on the
+    single-root and the batched paths."""
+    for fen in (START, MATED, STALEMATE):
+        p = pg.parse_fen(fen)
+        assert gpu_engine.perft_position(p, 0) == 1
+        for d in (1, 2, 3):
+            assert gpu_engine.perft_position(p, d) == oracle.perft(fen, d), (fen, d)
+    roots = [pg.parse_fen(f) for f in (START, MATED, STALEMATE, START)]
+    assert gpu_engine.perft_batch(roots, [0, 3, 2, 1]) == [1, 0, 0, 20]

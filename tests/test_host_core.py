@@ -132,3 +132,16 @@ def test_cli_batch_file_and_json(tmp_path):
     assert out.returncode == 2 and "MISMATCH" in out.stdout
     out = subprocess.run([cli, "-batch", str(f), "-cpu", "-strict"], capture_output=True, text=True)
     assert out.returncode == 0
+
+
+def test_host_edge_depths_and_terminal_positions(oracle):
+    eng = pg.Engine(device=-1)
+    mated = "rnb1kbnr/pppp1ppp/8/4p3/6Pq/5P2/PPPPP2P/RNBQKBNR w KQkq - 1 3"
+    stalemate = "7k/5Q2/6K1/8/8/8/8/8 b - - 0 1"
+    for fen in (pg.START_FEN, mated, stalemate):
+        p = pg.parse_fen(fen)
+        assert eng.perft_cpu(p, 0) == 1
+        for d in (1, 2, 3):
+            assert eng.perft_cpu(p, d) == oracle.perft(fen, d), (fen, d)
+    assert pg.count_moves(pg.parse_fen(mated)) == 0
+    assert pg.count_moves(pg.parse_fen(stalemate)) == 0
