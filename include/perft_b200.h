@@ -185,6 +185,14 @@ int pb_random_playouts(uint64_t seed, int n, int min_plies, int max_plies, pb_po
  * n u32 counts into n u64 offsets and a device u64 total. */
 int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total);
 
+/* Self-test of the device-side failure detection (no reference counterpart:
+ * the reference's waits are inside CUB).  Runs one tile of the scan whose
+ * predecessor never publishes: the look-back gives up after its bounded wait
+ * (about a second) and the kernel returns.  *device_error receives the error
+ * word (1 = scan wait timed out), *seconds (optional) the wait's wall time.
+ * Returns PB_OK when the launch completed; the context stays usable. */
+int pb_selftest_wait_timeout(pb_ctx *ctx, uint32_t *device_error, double *seconds);
+
 /* Learned scheduler network (no reference counterpart): 781 binary inputs
  * (12x64 piece-square, side to move, 4 castle rights, 8 en-passant files) ->
  * 256 -> 256 -> 4 outputs = predicted log2(1 + perft(k)), k = 1..4.  BF16

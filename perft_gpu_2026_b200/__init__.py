@@ -148,6 +148,7 @@ def _load() -> ctypes.CDLL:
         "pb_perft_batch_planned": (ctypes.c_int, [ctypes.c_void_p, P(Pos), P(ctypes.c_int), ctypes.c_int,
                                                    P(ctypes.c_uint64), P(PlanStats)]),
         "pb_dev_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
+        "pb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_uint32), P(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -448,6 +449,14 @@ class Engine:
         out = np.empty((n, 4), dtype=np.float32)
         self._check(lib.pb_mlp_predict(self._h, arr, n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
+
+    def selftest_wait_timeout(self):
+        """(device error word, seconds) of a scan tile whose predecessor never
+        publishes: the bounded wait gives up and reports 1."""
+        err = ctypes.c_uint32()
+        secs = ctypes.c_double()
+        self._check(lib.pb_selftest_wait_timeout(self._h, ctypes.byref(err), ctypes.byref(secs)))
+        return err.value, secs.value
 
     def dev_scan(self, d_in: int, n: int, d_out: int, d_total: int) -> None:
         self._check(lib.pb_dev_scan(self._h, ctypes.c_void_p(d_in), n, ctypes.c_void_p(d_out), ctypes.c_void_p(d_total)))

@@ -1723,6 +1723,36 @@ int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, 
     return PB_OK;
 }
 
+int pb_selftest_wait_timeout(pb_ctx *ctx, uint32_t *device_error, double *seconds)
+{
+    if (!ctx || !ctx->gpu || !device_error) return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    // two scan tiles, one CTA: it draws ticket 1, so tile 0 (whose prefix
+    // tile 1 waits for) is never published and the wait has to give up
+    const u64 n = 2 * (u64)SCAN_TILE;
+    Arena ar{ctx->arena, ctx->arena_bytes};
+    u32 *in = ar.take<u32>(n);
+    u64 *out = ar.take<u64>(n);
+    u64 *status = ar.take<u64>(2);
+    u64 *total = ar.take<u64>(1);
+    if (!in || !out || !status || !total) return fail(ctx, PB_ERR_NOMEM, "arena too small for the self-test");
+    PB_CUDA(cudaMemsetAsync(in, 0, sizeof(u32) * n, s));
+    PB_CUDA(cudaMemsetAsync(status, 0, 2 * sizeof(u64), s));
+    PB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s));
+    ctx->h_pinned[3] = 1;
+    PB_CUDA(cudaMemcpyAsync(ctx->d_ticket, &ctx->h_pinned[3], sizeof(u32), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    const auto t0 = std::chrono::steady_clock::now();
+    k_scan<<<1, SCAN_THREADS, 0, s>>>(in, n, out, status, ctx->d_ticket, total, ctx->d_err);
+    PB_CUDA(cudaGetLastError());
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 1, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *device_error = (u32)ctx->h_pinned[1];
+    return PB_OK;
+}
+
 int pb_scan_u32_noalloc(const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total, void *stream)
 {
     if (!d_in || !d_out || !d_total) return PB_ERR_ARG;

@@ -83,7 +83,7 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS = 32;  // a multiple of 8
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr u64 ST_AGG = 1ULL << 62, ST_PREFIX = 2ULL << 62, ST_VALUE = (1ULL << 62) - 1;
-constexpr u32 SCAN_SPIN_LIMIT = 1u << 22;
+constexpr u32 SCAN_SPIN_LIMIT = 1u << 20;  // look-back rounds (about a second) before giving up
 
 __device__ __forceinline__ void st_release(u64 *p, u64 v)
 {
