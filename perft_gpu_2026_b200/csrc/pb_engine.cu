@@ -22,6 +22,7 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
 #include "../../include/perft_b200.h"
 #include "pb_tables.cuh"
 #include "pb_util.cuh"
@@ -176,6 +177,16 @@ struct Arena {
 
 inline unsigned grid_for(u64 n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
+// NVTX range for profilers (header-only NVTX v3: free unless a tool attaches):
+// marks each BFS pass, level and leaf launch on the host timeline, so a
+// capture can select kernels by phase (ncu --nvtx --nvtx-include).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 enum { BFS_OK = 0, BFS_TOO_BIG = 1 };
 
 template <int C, bool S>
@@ -252,6 +263,7 @@ void launch_generate(pb_ctx *ctx, int c, const Board *b, const uint8_t *st, cons
 // One GPU breadth-first perft; status BFS_TOO_BIG when a level would not fit.
 int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth, u64 *out, int *bfs_status)
 {
+    NvtxRange nvtx_pass("bfs_perft");
     *bfs_status = BFS_OK;
     const bool strict = ctx->opts.strict != 0;
     if (depth <= 2) {
@@ -347,7 +359,11 @@ int bfs_perft(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth,
     }
     PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(unsigned long long), s));
     if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[1], s));
-    int rc = launch_leaf(ctx, c, strict, cur_b, cur_s, epi, emv, n, n_par);
+    int rc;
+    {
+        NvtxRange nvtx_leaf("leaf");
+        rc = launch_leaf(ctx, c, strict, cur_b, cur_s, epi, emv, n, n_par);
+    }
     if (rc != PB_OK) return rc;
     PB_CUDA(cudaGetLastError());
     if (ctx->timing) {
@@ -404,6 +420,7 @@ struct TTLevel {
 int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth, const Hash128 &root_hash,
                  u64 *out, int *bfs_status)
 {
+    NvtxRange nvtx_pass("bfs_perft_tt");
     *bfs_status = BFS_OK;
     const bool strict = ctx->opts.strict != 0;
     if (depth <= 2) {
@@ -653,6 +670,7 @@ inline void to_white_to_move(const pb_pos &p, Board &b, uint8_t &st)
 // out[i] = perft(depth) of root i.  BFS_TOO_BIG when a level does not fit.
 int bfs_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth, u64 *out, int *bfs_status)
 {
+    NvtxRange nvtx_pass("bfs_batch");
     *bfs_status = BFS_OK;
     const bool strict = ctx->opts.strict != 0;
     if (n == 0) return PB_OK;
@@ -1044,6 +1062,7 @@ int capture_batch_graph(pb_ctx *ctx, GraphPlan &g)
 int run_planned_batch(pb_ctx *ctx, GraphPlan &g, const Board *rb, const uint8_t *rs, u64 n, int depth,
                       const std::vector<u64> &caps, u64 *out, bool *overflow)
 {
+    NvtxRange nvtx_pass("planned_batch");
     *overflow = false;
     const bool strict = ctx->opts.strict != 0;
     const bool sort = ctx->tuning.leaf_kernel == 4;
