@@ -372,6 +372,11 @@ class Engine:
 
     def set_tuning(self, leaf_kernel: int = 0, leaf_blocks_per_sm: int = 0, leaf_threads: int = 0,
                    gen_threads: int = 0, leaf_fuse: int = 0, tt_replace: int = 0) -> None:
+        """Launch parameters (pb_set_tuning); 0 keeps the current value.
+        leaf_kernel 1 = one edge per thread, 2 = cooperative, 3 = in-check
+        children deferred, 4 = children ranked by move count (default);
+        leaf_threads 128/256/512; gen_threads 64/128; leaf_fuse 1/2;
+        tt_replace 1 = always overwrite, 2 = two-slot size priority."""
         t = Tuning()
         t.tt_replace = tt_replace
         t.leaf_kernel = leaf_kernel
