@@ -73,7 +73,12 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        # raw samples go to $BENCH_CLOCKS_DIR (default: the temp directory);
+        # the JSON line carries their summary
+        import tempfile
+
+        out_dir = os.environ.get("BENCH_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"clocks_bench_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
