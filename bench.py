@@ -32,6 +32,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -75,8 +76,6 @@ class ClockSampler:
         self.proc = None
         # raw samples go to $BENCH_CLOCKS_DIR (default: the temp directory);
         # the JSON line carries their summary
-        import tempfile
-
         out_dir = os.environ.get("BENCH_CLOCKS_DIR") or tempfile.gettempdir()
         self.path = os.path.join(out_dir, f"clocks_bench_{os.getpid()}.csv")
 
