@@ -385,6 +385,12 @@ def main():
             roofline["achieved"] = ach
             roofline["frac"] = ach / issue_peak
             roofline["inst_per_position"] = inst_per_pos
+        if consts.get("ncu_alu_pipe_pct"):
+            # the binding unit: the integer ALU pipe runs at half the issue
+            # rate, so the issue fraction cannot reach 1 with this mix
+            roofline["binding_unit"] = {"unit": "ALU pipe", "util_pct": consts["ncu_alu_pipe_pct"],
+                                        "issue_active_pct": consts.get("ncu_issue_active_pct"),
+                                        "source": "ncu --set full capture of the same kernel (profiles/)"}
         line = {"metric": METRIC, "value": nodes / (my_ms / 1e3), "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": my_ms, "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
