@@ -145,3 +145,19 @@ def test_host_edge_depths_and_terminal_positions(oracle):
             assert eng.perft_cpu(p, d) == oracle.perft(fen, d), (fen, d)
     assert pg.count_moves(pg.parse_fen(mated)) == 0
     assert pg.count_moves(pg.parse_fen(stalemate)) == 0
+
+
+def test_cli_flags_anywhere_and_positional_launch_depth():
+    """The reference's argument handling: flags may come before, between or
+    after the positional arguments, and a third positional is the launch
+    depth; every form counts the same."""
+    import os
+    import subprocess
+    cli = os.path.join(os.path.dirname(pg.__file__), "perft_gpu")
+    kiwi = "r3k2r/p1ppqpb1/bn2pnp1/3PN3/1p2P3/2N2Q1p/PPPBBPPP/R3K2R w KQkq -"
+    want = ["Perft(01): 48", "Perft(02): 2039", "Perft(03): 97862"]
+    for argv in ([kiwi, "3", "-cpu", "-nott"], ["-cpu", kiwi, "-nott", "3"], ["-nott", "-cpu", kiwi, "3", "2"],
+                 [kiwi, "-ld", "2", "3", "-cpu"]):
+        out = subprocess.run([cli] + argv, capture_output=True, text=True, check=True).stdout
+        got = [l.split(",")[0] for l in out.splitlines() if l.startswith("Perft(")]
+        assert got == want, argv
