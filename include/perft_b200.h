@@ -185,6 +185,22 @@ int pb_random_playouts(uint64_t seed, int n, int min_plies, int max_plies, pb_po
  * n u32 counts into n u64 offsets and a device u64 total. */
 int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total);
 
+/* The BFS level kernels on caller-owned device buffers, for unit tests
+ * against the host functions.  Boards are 4 x u64 (the pb_pos bitboards),
+ * 32-byte aligned; color = side to move at the parents.
+ * pb_dev_expand: child i = parent d_pidx[i] after move d_moves[i]; writes its
+ * board, state and exact legal-move count (makemove_and_count_moves_kernel,
+ * perft_kernels.cu:201-257).
+ * pb_dev_generate: the moves of parent j go to [d_offs[j], d_offs[j+1]) (the
+ * last ends at *d_total) as (move, parent j), in the generator's order
+ * (generate_moves_kernel + mp_interval_expand_kernel, perft_kernels.cu:77-173,
+ * :263-311); the offsets must come from the exact counts. */
+int pb_dev_expand(pb_ctx *ctx, const void *d_boards, const uint8_t *d_states, int color, const uint32_t *d_pidx,
+                  const uint16_t *d_moves, uint64_t n, uint64_t nparents, void *d_child_boards,
+                  uint8_t *d_child_states, uint32_t *d_counts);
+int pb_dev_generate(pb_ctx *ctx, const void *d_boards, const uint8_t *d_states, int color, const uint64_t *d_offs,
+                    const uint64_t *d_total, uint64_t n, uint16_t *d_moves, uint32_t *d_pidx);
+
 /* Self-test of the device-side failure detection (no reference counterpart:
  * the reference's waits are inside CUB).  Runs one tile of the scan whose
  * predecessor never publishes: the look-back gives up after its bounded wait

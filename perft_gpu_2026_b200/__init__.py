@@ -149,6 +149,12 @@ def _load() -> ctypes.CDLL:
                                                    P(ctypes.c_uint64), P(PlanStats)]),
         "pb_dev_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
         "pb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_uint32), P(ctypes.c_double)]),
+        "pb_dev_expand": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
+        "pb_dev_generate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -454,6 +460,17 @@ class Engine:
         out = np.empty((n, 4), dtype=np.float32)
         self._check(lib.pb_mlp_predict(self._h, arr, n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
+
+    def dev_expand(self, d_boards: int, d_states: int, color: int, d_pidx: int, d_moves: int, n: int, nparents: int,
+                   d_child_boards: int, d_child_states: int, d_counts: int) -> None:
+        """The make+count level kernel on caller-owned device buffers (tests)."""
+        self._check(lib.pb_dev_expand(self._h, d_boards, d_states, color, d_pidx, d_moves, n, nparents, d_child_boards,
+                                      d_child_states, d_counts))
+
+    def dev_generate(self, d_boards: int, d_states: int, color: int, d_offs: int, d_total: int, n: int, d_moves: int,
+                     d_pidx: int) -> None:
+        """The staged generation kernel on caller-owned device buffers (tests)."""
+        self._check(lib.pb_dev_generate(self._h, d_boards, d_states, color, d_offs, d_total, n, d_moves, d_pidx))
 
     def selftest_wait_timeout(self):
         """(device error word, seconds) of a scan tile whose predecessor never

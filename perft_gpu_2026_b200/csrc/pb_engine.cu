@@ -1742,6 +1742,63 @@ int pb_dev_scan(pb_ctx *ctx, const uint32_t *d_in, uint64_t n, uint64_t *d_out, 
     return PB_OK;
 }
 
+// Finishes a test launch: waits, reads the error word.
+static int finish_test_launch(pb_ctx *ctx, const char *what)
+{
+    cudaStream_t s = ctx->stream;
+    PB_CUDA(cudaGetLastError());
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 1, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    if ((u32)ctx->h_pinned[1]) return fail(ctx, PB_ERR_DEVICE, what);
+    return PB_OK;
+}
+
+int pb_dev_expand(pb_ctx *ctx, const void *d_boards, const uint8_t *d_states, int color, const uint32_t *d_pidx,
+                  const uint16_t *d_moves, uint64_t n, uint64_t nparents, void *d_child_boards,
+                  uint8_t *d_child_states, uint32_t *d_counts)
+{
+    if (!ctx || !ctx->gpu || !d_boards || !d_states || !d_pidx || !d_moves || !d_child_boards || !d_child_states ||
+        !d_counts || (color != WHITE && color != BLACK))
+        return PB_ERR_ARG;
+    if (((uintptr_t)d_boards | (uintptr_t)d_child_boards) & 31) return PB_ERR_ARG;  // 256-bit accesses
+    if (n == 0) return PB_OK;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    PB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s));
+    const Board *pb_ = static_cast<const Board *>(d_boards);
+    Board *cb = static_cast<Board *>(d_child_boards);
+    if (color == WHITE)
+        k_expand_count<WHITE><<<grid_for(n, 256), 256, 0, s>>>(pb_, d_states, d_pidx, d_moves, n, nparents, cb,
+                                                               d_child_states, d_counts, ctx->d_err);
+    else
+        k_expand_count<BLACK><<<grid_for(n, 256), 256, 0, s>>>(pb_, d_states, d_pidx, d_moves, n, nparents, cb,
+                                                               d_child_states, d_counts, ctx->d_err);
+    return finish_test_launch(ctx, "make+count kernel reported a device error");
+}
+
+int pb_dev_generate(pb_ctx *ctx, const void *d_boards, const uint8_t *d_states, int color, const uint64_t *d_offs,
+                    const uint64_t *d_total, uint64_t n, uint16_t *d_moves, uint32_t *d_pidx)
+{
+    if (!ctx || !ctx->gpu || !d_boards || !d_states || !d_offs || !d_total || !d_moves || !d_pidx ||
+        (color != WHITE && color != BLACK))
+        return PB_ERR_ARG;
+    if ((uintptr_t)d_boards & 31) return PB_ERR_ARG;
+    if (n == 0) return PB_OK;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    PB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s));
+    const Board *pb_ = static_cast<const Board *>(d_boards);
+    const u64 *offs = reinterpret_cast<const u64 *>(d_offs);
+    const u64 *total = reinterpret_cast<const u64 *>(d_total);
+    if (color == WHITE)
+        k_generate<WHITE, GEN_THREADS><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(pb_, d_states, offs, total, n,
+                                                                                      d_moves, d_pidx, ctx->d_err);
+    else
+        k_generate<BLACK, GEN_THREADS><<<grid_for(n, GEN_THREADS), GEN_THREADS, 0, s>>>(pb_, d_states, offs, total, n,
+                                                                                      d_moves, d_pidx, ctx->d_err);
+    return finish_test_launch(ctx, "generation kernel reported a device error");
+}
+
 int pb_selftest_wait_timeout(pb_ctx *ctx, uint32_t *device_error, double *seconds)
 {
     if (!ctx || !ctx->gpu || !device_error) return PB_ERR_ARG;
