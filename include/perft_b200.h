@@ -126,6 +126,13 @@ int pb_count_moves(const pb_pos *pos, int strict);
 int pb_generate_moves(const pb_pos *pos, uint16_t *moves);
 int pb_make_move(pb_pos *pos, uint16_t move);
 
+/* 128-bit Zobrist key of a position (computeHash, zobrist.h:81-147), and the
+ * key after `move` updated incrementally from the parent's key
+ * (updateHashAfterMove, zobrist.h:149-227): the keys the transposition tables
+ * use, on host and device alike. */
+int pb_position_hash(const pb_pos *pos, pb_u128 *out);
+int pb_hash_after_move(const pb_u128 *key, const pb_pos *pos, uint16_t move, pb_u128 *out);
+
 /* Workload generator (no reference counterpart): a playout of `plies`
  * uniformly random legal moves from the standard initial array; each move is
  * drawn with splitmix64 (state advanced in place) among the legal moves sorted

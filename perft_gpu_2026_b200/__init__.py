@@ -126,6 +126,8 @@ def _load() -> ctypes.CDLL:
         "pb_count_moves": (ctypes.c_int, [P(Pos), ctypes.c_int]),
         "pb_generate_moves": (ctypes.c_int, [P(Pos), P(ctypes.c_uint16)]),
         "pb_make_move": (ctypes.c_int, [P(Pos), ctypes.c_uint16]),
+        "pb_position_hash": (ctypes.c_int, [P(Pos), P(U128)]),
+        "pb_hash_after_move": (ctypes.c_int, [P(U128), P(Pos), ctypes.c_uint16, P(U128)]),
         "pb_random_playout": (ctypes.c_int, [P(ctypes.c_uint64), ctypes.c_int, P(Pos)]),
         "pb_random_playouts": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(Pos),
                                                P(ctypes.c_int)]),
@@ -216,6 +218,21 @@ def make_move(p: Pos, move: int) -> Pos:
     ctypes.memmove(ctypes.byref(q), ctypes.byref(p), ctypes.sizeof(Pos))
     lib.pb_make_move(ctypes.byref(q), move)
     return q
+
+
+def position_hash(p: Pos) -> int:
+    """128-bit Zobrist key of the position (as one Python int)."""
+    out = U128()
+    lib.pb_position_hash(ctypes.byref(p), ctypes.byref(out))
+    return out.value()
+
+
+def hash_after_move(key: int, p: Pos, move: int) -> int:
+    """Key after `move`, updated incrementally from `key` (the key of p)."""
+    k = U128(key & ((1 << 64) - 1), key >> 64)
+    out = U128()
+    lib.pb_hash_after_move(ctypes.byref(k), ctypes.byref(p), move, ctypes.byref(out))
+    return out.value()
 
 
 def move_uci(m: int) -> str:

@@ -1494,6 +1494,30 @@ int pb_generate_moves(const pb_pos *pos, uint16_t *moves)
     return host_gen(to_board(*pos), pos->state, pos->color, moves);
 }
 
+int pb_position_hash(const pb_pos *pos, pb_u128 *out)
+{
+    if (!pos || !out) return PB_ERR_ARG;
+    build_zobrist();
+    const Hash128 h = hash_position(to_board(*pos), pos->state, pos->color);
+    out->lo = h.lo;
+    out->hi = h.hi;
+    return PB_OK;
+}
+
+int pb_hash_after_move(const pb_u128 *key, const pb_pos *pos, uint16_t move, pb_u128 *out)
+{
+    if (!key || !pos || !out) return PB_ERR_ARG;
+    build_zobrist();
+    const Board b = to_board(*pos);
+    Board after = b;
+    u32 st = pos->state;
+    host_make(after, st, pos->color, move);
+    const Hash128 h = hash_move(Hash128{key->lo, key->hi}, b, pos->state, st, pos->color, move);
+    out->lo = h.lo;
+    out->hi = h.hi;
+    return PB_OK;
+}
+
 int pb_make_move(pb_pos *pos, uint16_t move)
 {
     if (!pos) return PB_ERR_ARG;

@@ -161,3 +161,40 @@ def test_cli_flags_anywhere_and_positional_launch_depth():
         out = subprocess.run([cli] + argv, capture_output=True, text=True, check=True).stdout
         got = [l.split(",")[0] for l in out.splitlines() if l.startswith("Perft(")]
         assert got == want, argv
+
+
+def test_incremental_hash_equals_full_hash_along_playouts():
+    """The key after every move, updated from the parent's key, equals the key
+    computed from scratch - over playouts long enough to meet castling, en
+    passant, promotions and captures - and different move orders reaching the
+    same position give the same key."""
+    seen_flags = set()
+    st = 8080
+    for game in range(300):
+        p = pg.parse_fen(pg.START_FEN)
+        key = pg.position_hash(p)
+        for ply in range(160):
+            moves = pg.generate_moves(p)
+            if not moves:
+                break
+            r, st = pg.splitmix64(st)
+            m = moves[r % len(moves)]
+            seen_flags.add(m >> 12)
+            key = pg.hash_after_move(key, p, m)
+            p = pg.make_move(p, m)
+            assert key == pg.position_hash(p), (game, ply, pg.to_fen(p))
+    assert {1, 2, 3, 5}.issubset(seen_flags) and any(f & 8 for f in seen_flags), seen_flags
+    # transposition: 1.Nf3 Nf6 2.Nc3 Nc6 and 1.Nc3 Nc6 2.Nf3 Nf6
+    def play(ucis):
+        p = pg.parse_fen(pg.START_FEN)
+        key = pg.position_hash(p)
+        for u in ucis:
+            m = next(m for m in pg.generate_moves(p) if pg.move_uci(m) == u)
+            key = pg.hash_after_move(key, p, m)
+            p = pg.make_move(p, m)
+        return key, p.key()
+    a, pa = play(["g1f3", "g8f6", "b1c3", "b8c6"])
+    b, pb = play(["b1c3", "b8c6", "g1f3", "g8f6"])
+    assert pa == pb and a == b
+    c, _ = play(["g1f3", "g8f6", "b1c3", "b8a6"])
+    assert c != a
