@@ -151,6 +151,7 @@ def _load() -> ctypes.CDLL:
                                                    P(ctypes.c_uint64), P(PlanStats)]),
         "pb_dev_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
         "pb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_uint32), P(ctypes.c_double)]),
+        "pb_selftest_tt_race": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, P(ctypes.c_uint64), P(ctypes.c_uint64)]),
         "pb_dev_expand": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p]),
@@ -488,6 +489,13 @@ class Engine:
                      d_pidx: int) -> None:
         """The staged generation kernel on caller-owned device buffers (tests)."""
         self._check(lib.pb_dev_generate(self._h, d_boards, d_states, color, d_offs, d_total, n, d_moves, d_pidx))
+
+    def selftest_tt_race(self, deep: bool):
+        """(wrong hits, hits) of the device-table race self-test."""
+        bad = ctypes.c_uint64()
+        hits = ctypes.c_uint64()
+        self._check(lib.pb_selftest_tt_race(self._h, int(deep), ctypes.byref(bad), ctypes.byref(hits)))
+        return bad.value, hits.value
 
     def selftest_wait_timeout(self):
         """(device error word, seconds) of a scan tile whose predecessor never

@@ -110,6 +110,44 @@ __device__ __forceinline__ void tt_store(const TTView &t, const Hash128 &h, u64 
         tt_write(t, slot + 1, h, count);
 }
 
+// Race self-test: every thread stores and probes keys of a small key set in
+// a table far smaller than the set, so stores and probes of different keys
+// hit the same slots at the same time.  Each key's count is a function of the
+// key; a probe that reports a hit with any other count (a torn or foreign
+// entry accepted) increments *bad.  No waits; every slot index is in range.
+__device__ __forceinline__ u64 race_mix(u64 z)
+{
+    // splitmix64 output function (Steele, Lea and Flood 2014)
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ Hash128 race_key(u32 k)
+{
+    Hash128 h;
+    h.lo = race_mix(0x9E3779B97F4A7C15ULL * (2ULL * k + 1));
+    h.hi = race_mix(0xD1B54A32D192ED03ULL * (2ULL * k + 2));
+    return h;
+}
+__device__ __forceinline__ u64 race_count(const Hash128 &h) { return (h.lo ^ (h.hi >> 7)) & 0xFFFFFULL; }
+__global__ void k_tt_race(TTView t, u32 nkeys, u32 iters, unsigned long long *bad, unsigned long long *hits)
+{
+    const u32 tid = blockIdx.x * blockDim.x + threadIdx.x;
+    u64 wrong = 0, seen = 0;
+    for (u32 it = 0; it < iters; it++) {
+        const Hash128 a = race_key((tid * 2654435761u + it * 40503u) % nkeys);
+        tt_store(t, a, race_count(a));
+        const Hash128 b = race_key((tid * 97u + it * 7919u + 1u) % nkeys);
+        u64 c;
+        if (tt_probe(t, b, &c)) {
+            seen++;
+            if (c != race_count(b)) wrong++;
+        }
+    }
+    if (wrong) atomicAdd(bad, (unsigned long long)wrong);
+    if (seen) atomicAdd(hits, (unsigned long long)seen);
+}
+
 struct TTViews {
     TTView v[TT_MAX_DEPTH];
 };

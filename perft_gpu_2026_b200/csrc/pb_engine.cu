@@ -1823,6 +1823,28 @@ int pb_dev_generate(pb_ctx *ctx, const void *d_boards, const uint8_t *d_states, 
     return finish_test_launch(ctx, "generation kernel reported a device error");
 }
 
+int pb_selftest_tt_race(pb_ctx *ctx, int deep, uint64_t *bad, uint64_t *hits)
+{
+    if (!ctx || !ctx->gpu || !bad || !hits) return PB_ERR_ARG;
+    PB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const u64 slots = 1024;  // far fewer slots than keys: constant collisions
+    Arena ar{ctx->arena, ctx->arena_bytes};
+    u64 *entries = ar.take<u64>(slots * (deep ? 4 : 2));
+    unsigned long long *cnt = ar.take<unsigned long long>(2);
+    if (!entries || !cnt) return fail(ctx, PB_ERR_NOMEM, "arena too small for the self-test");
+    PB_CUDA(cudaMemsetAsync(entries, 0, slots * (deep ? 32 : 16), s));
+    PB_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), s));
+    const TTView t{entries, slots, deep ? TT_DEEP : TT_SHALLOW, 0};
+    k_tt_race<<<4 * ctx->num_sms, 256, 0, s>>>(t, 8192, 64, cnt, cnt + 1);
+    PB_CUDA(cudaGetLastError());
+    PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, cnt, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    *bad = ctx->h_pinned[0];
+    *hits = ctx->h_pinned[1];
+    return PB_OK;
+}
+
 int pb_selftest_wait_timeout(pb_ctx *ctx, uint32_t *device_error, double *seconds)
 {
     if (!ctx || !ctx->gpu || !device_error) return PB_ERR_ARG;

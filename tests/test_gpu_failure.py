@@ -18,3 +18,13 @@ def test_scan_wait_gives_up_and_reports(gpu_engine):
     assert gpu_engine.perft_position(pg.parse_fen(pg.START_FEN), 5) == 4_865_609
     err2, _ = gpu_engine.selftest_wait_timeout()
     assert err2 == DEVERR_SCAN_TIMEOUT
+
+
+@pytest.mark.parametrize("deep", [False, True])
+def test_device_table_races_never_return_a_foreign_count(gpu_engine, deep):
+    """Stores and probes of colliding keys from every thread at once: a probe
+    either misses or returns its own key's count (the XOR lock and the full
+    key check reject torn and foreign entries)."""
+    bad, hits = gpu_engine.selftest_tt_race(deep)
+    assert hits > 1000
+    assert bad == 0
