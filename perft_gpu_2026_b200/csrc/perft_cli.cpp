@@ -1,6 +1,7 @@
 // perft_cli.cpp - the perft_gpu command line on top of the C ABI.
 //
 //   perft_gpu <fen> <depth> [<launchdepth>] [-nott] [-dtt <MB>] [-htt <MB>] [-ld <N>] [-cpu] [-strict] [-json]
+//             [-journal <file>]
 //   perft_gpu -batch <file> [<depth>] [-cpu] [-strict] [-json]
 //
 // Same surface and output as the reference program (perft.cu:13-186):
@@ -13,7 +14,10 @@
 // file of positions, one per line: a FEN followed by optional ";D<k> <count>"
 // expected counts (EPD-style); every depth up to the largest listed (or the
 // <depth> argument) runs as one batched GPU pass over all positions, and
-// mismatches against the listed counts are reported.
+// mismatches against the listed counts are reported.  -journal <file> makes
+// a long run resumable: the final depth runs root move by root move, each
+// finished subtree is appended to the file, and a rerun with the same file,
+// FEN and depth skips the moves already recorded there.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -158,10 +162,92 @@ static int run_batch(const std::string &path, int depth_arg, bool cpu, bool json
     return bad ? 2 : 0;
 }
 
+static std::string move_text(uint16_t m)
+{
+    const char *files = "abcdefgh";
+    int f = m & 63, t = (m >> 6) & 63, fl = m >> 12;
+    std::string out;
+    out += files[f & 7];
+    out += char('1' + (f >> 3));
+    out += files[t & 7];
+    out += char('1' + (t >> 3));
+    if (fl & 8) out += "nbrq"[fl & 3];
+    return out;
+}
+
+static pb_u128 add_u128(pb_u128 a, uint64_t b)
+{
+    pb_u128 r{a.lo + b, a.hi};
+    if (r.lo < a.lo) r.hi++;
+    return r;
+}
+
+// The final depth, one root move at a time, with the journal file: lines
+// "<depth> <move> <count> <fen>" for finished subtrees.  Recorded moves of the
+// same FEN and depth are read back instead of recomputed; every subtree
+// finished here is appended (and flushed) as soon as it is known.
+static int journaled_depth(pb_ctx *ctx, const pb_pos &root, const std::string &fen, int depth,
+                           const std::string &path, pb_u128 *total, double *secs, int *reused)
+{
+    std::vector<std::pair<std::string, uint64_t>> done;
+    {
+        std::ifstream in(path);
+        std::string line;
+        while (std::getline(in, line)) {
+            std::istringstream ls(line);
+            int d;
+            std::string mv, f, rest;
+            unsigned long long c;
+            if (!(ls >> d >> mv >> c)) continue;
+            std::getline(ls, rest);
+            f = rest.substr(rest.find_first_not_of(' ') == std::string::npos ? 0 : rest.find_first_not_of(' '));
+            if (d == depth && f == fen) done.emplace_back(mv, c);
+        }
+    }
+    FILE *out = fopen(path.c_str(), "a");
+    if (!out) {
+        fprintf(stderr, "cannot open journal %s\n", path.c_str());
+        return PB_ERR_ARG;
+    }
+    uint16_t moves[256];
+    int n = pb_generate_moves(&root, moves);
+    *total = pb_u128{0, 0};
+    *reused = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    for (int i = 0; i < n; i++) {
+        const std::string mt = move_text(moves[i]);
+        auto hit = std::find_if(done.begin(), done.end(), [&](const auto &e) { return e.first == mt; });
+        if (hit != done.end()) {
+            *total = add_u128(*total, hit->second);
+            (*reused)++;
+            continue;
+        }
+        pb_pos child = root;
+        pb_make_move(&child, moves[i]);
+        pb_u128 v;
+        double s = 0;
+        int rc = pb_perft_launch(ctx, &child, depth - 1, &v, &s);
+        if (rc != PB_OK) {
+            fclose(out);
+            return rc;
+        }
+        if (v.hi) {  // a subtree above 2^64 is not journalled; count it all the same
+            total->hi += v.hi;
+        } else {
+            fprintf(out, "%d %s %llu %s\n", depth, mt.c_str(), (unsigned long long)v.lo, fen.c_str());
+            fflush(out);
+        }
+        *total = add_u128(*total, v.lo);
+    }
+    fclose(out);
+    *secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return PB_OK;
+}
+
 int main(int argc, char **argv)
 {
     bool cpu = false, json = false;
-    std::string batch_file;
+    std::string batch_file, journal;
     pb_opts opts;
     pb_default_opts(&opts);
     std::vector<std::string> pos;
@@ -172,6 +258,7 @@ int main(int argc, char **argv)
         else if (a == "-strict") opts.strict = 1;
         else if (a == "-json") json = true;
         else if (a == "-batch" && i + 1 < argc) batch_file = argv[++i];
+        else if (a == "-journal" && i + 1 < argc) journal = argv[++i];
         else if (a == "-ld" && i + 1 < argc) opts.launch_depth = atoi(argv[++i]);
         else if (a == "-dtt" && i + 1 < argc) opts.device_tt_mb = atoi(argv[++i]);
         else if (a == "-htt" && i + 1 < argc) opts.host_tt_mb = atoi(argv[++i]);
@@ -185,7 +272,8 @@ int main(int argc, char **argv)
         max_depth = atoi(pos[1].c_str());
         if (pos.size() >= 3 && opts.launch_depth == 0) opts.launch_depth = atoi(pos[2].c_str());
     } else {
-        printf("\nUsage: perft_gpu <fen> <depth> [<launchdepth>] [-nott] [-dtt <MB>] [-htt <MB>] [-ld <N>] [-cpu] [-strict]\n");
+        printf("\nUsage: perft_gpu <fen> <depth> [<launchdepth>] [-nott] [-dtt <MB>] [-htt <MB>] [-ld <N>] [-cpu] [-strict]"
+               " [-json] [-journal <file>]\n");
         printf("\nAs no parameters were provided... running default test\n");
     }
     pb_pos root;
@@ -206,7 +294,11 @@ int main(int argc, char **argv)
         for (int d = 1; d <= max_depth; d++) {
             pb_u128 v;
             double secs = 0;
-            int rc = pb_perft_launch(ctx, &root, d, &v, &secs);
+            int reused = 0;
+            int rc = (!journal.empty() && d == max_depth && d > 1)
+                         ? journaled_depth(ctx, root, fen, d, journal, &v, &secs, &reused)
+                         : pb_perft_launch(ctx, &root, d, &v, &secs);
+            if (reused) printf("\njournal: %d root moves read back from %s\n", reused, journal.c_str());
             if (rc != PB_OK) {
                 fprintf(stderr, "error: %s\n", pb_last_error(ctx));
                 return 1;
@@ -234,7 +326,10 @@ int main(int argc, char **argv)
     for (int d = 1; d <= max_depth; d++) {
         pb_u128 v;
         double secs = 0;
-        rc = pb_perft_launch(ctx, &root, d, &v, &secs);
+        int reused = 0;
+        rc = (!journal.empty() && d == max_depth && d > 1) ? journaled_depth(ctx, root, fen, d, journal, &v, &secs, &reused)
+                                                           : pb_perft_launch(ctx, &root, d, &v, &secs);
+        if (reused) printf("\njournal: %d root moves read back from %s\n", reused, journal.c_str());
         if (rc != PB_OK) {
             fprintf(stderr, "error: %s\n", pb_last_error(ctx));
             pb_destroy(ctx);

@@ -198,3 +198,30 @@ def test_incremental_hash_equals_full_hash_along_playouts():
     assert pa == pb and a == b
     c, _ = play(["g1f3", "g8f6", "b1c3", "b8a6"])
     assert c != a
+
+
+def test_cli_journal_resumes_a_partial_run(tmp_path):
+    """-journal: a run records every root move's subtree at the final depth;
+    a rerun after losing part of the file recomputes only the missing moves
+    and prints the same totals."""
+    import os
+    import subprocess
+    cli = os.path.join(os.path.dirname(pg.__file__), "perft_gpu")
+    kiwi = "r3k2r/p1ppqpb1/bn2pnp1/3PN3/1p2P3/2N2Q1p/PPPBBPPP/R3K2R w KQkq -"
+    j = tmp_path / "run.journal"
+
+    def run():
+        out = subprocess.run([cli, kiwi, "4", "-cpu", "-journal", str(j)], capture_output=True, text=True,
+                             check=True).stdout
+        lines = [l.split(",")[0] for l in out.splitlines() if l.startswith("Perft(")]
+        return lines, out
+
+    want = ["Perft(01): 48", "Perft(02): 2039", "Perft(03): 97862", "Perft(04): 4085603"]
+    lines, out = run()
+    assert lines == want and "read back" not in out
+    rec = j.read_text().splitlines()
+    assert len(rec) == 48 and all(r.startswith("4 ") and r.endswith(kiwi) for r in rec)
+    j.write_text("\n".join(rec[:20] + ["3 a2a3 999 " + kiwi]) + "\n")  # an interrupted run (+ another depth)
+    lines, out = run()
+    assert lines == want and "journal: 20 root moves read back" in out
+    assert len([r for r in j.read_text().splitlines() if r.startswith("4 ")]) == 48
