@@ -244,3 +244,18 @@ def test_edge_depths_and_terminal_positions(gpu_engine, oracle):
             assert gpu_engine.perft_position(p, d) == oracle.perft(fen, d), (fen, d)
     roots = [pg.parse_fen(f) for f in (START, MATED, STALEMATE, START)]
     assert gpu_engine.perft_batch(roots, [0, 3, 2, 1]) == [1, 0, 0, 20]
+
+
+def test_batched_leaf_ranked_and_unranked_agree():
+    """The batched leaf with and without ranking each CTA's children by move
+    count (leaf_kernel 4 / 1), on uneven roots, both colours to move."""
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
+    roots = pg.uneven_roots(192, 6, 40, seed=23)
+    depths = [2 + (i % 4) for i in range(len(roots))]
+    eng.set_tuning(leaf_kernel=4)
+    ranked = eng.perft_batch(roots, depths)
+    eng.set_tuning(leaf_kernel=1)
+    plain = eng.perft_batch(roots, depths)
+    assert ranked == plain
+    assert ranked == [eng.perft_position(r, d) for r, d in zip(roots, depths)]
+    eng.close()

@@ -93,3 +93,13 @@ def test_trained_network_plans_a_tight_arena_better_than_a_constant_guess():
     assert res["trained"][1] == 0, res
     assert res["constant"][1] >= res["trained"][1], res
     assert res["trained"][0] < 0.8 * res["constant"][0], res
+
+
+def test_planned_batch_strict_mode_matches_strict_per_root():
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30, strict=True)
+    _train(eng, n=1024)
+    roots = pg.uneven_roots(96, 6, 40, seed=21)
+    depths = [3 + (i % 3) for i in range(len(roots))]
+    got, _ = eng.perft_batch_planned(roots, depths)
+    assert got == [eng.perft_position(r, d) for r, d in zip(roots, depths)]
+    eng.close()
