@@ -111,6 +111,15 @@ int pb_perft_launch(pb_ctx *ctx, const pb_pos *pos, int depth, pb_u128 *count, d
  * cumulative per-depth results and wall times. */
 int pb_perft(pb_ctx *ctx, const char *fen, int max_depth, pb_u128 *per_depth, double *per_depth_secs);
 
+/* 128-bit counts (uint128.h:13-108).  pb_u128_add is the accumulation the
+ * host recursion above the launch depth applies to every subtree count
+ * (perft_cpu_recurse, launcher.cu:570-571, 700-705): *acc += *v with the
+ * carry into the high word.  pb_u128_text writes the decimal text of *v
+ * (uint128::toDecimalString, uint128.h:46-108) into buf; returns the text
+ * length, or PB_ERR_ARG when buf holds fewer than 40 bytes. */
+void pb_u128_add(pb_u128 *acc, const pb_u128 *v);
+int pb_u128_text(const pb_u128 *v, char *buf, size_t len);
+
 /* Replaces perft_cpu_dispatch (launcher.cu:807-816): host-only perft. */
 int pb_perft_cpu(pb_ctx *ctx, const pb_pos *pos, int depth, uint64_t *count);
 
@@ -269,8 +278,12 @@ int pb_perft_batch_planned(pb_ctx *ctx, const pb_pos *roots, const int *depths, 
  *     many scan tiles); larger n returns PB_ERR_ARG without touching the GPU.
  *   - Runs on `stream` (NULL = default stream) of the current device and waits
  *     for it before returning; n == 0 returns PB_OK and writes nothing.
- *   - The first call on a device looks up the array's device address (set-up);
- *     make that first call before any stream capture.
+ *   - Because it waits for its stream, it cannot run inside a stream capture:
+ *     a call on a capturing stream returns PB_ERR_ARG and records nothing.
+ *   - Every call looks up the array's device address with the caller's device
+ *     current (the lookup allocates nothing; the first call on a device also
+ *     loads the library's module there).
+ *   - The array is 8.25 KB per device and stays until the process exits.
  *   - All calls share the one array, so calls that overlap on the GPU (other
  *     threads or streams of the same device) race; serialise them. */
 int pb_scan_u32_noalloc(const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *d_total, void *stream);

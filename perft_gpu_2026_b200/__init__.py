@@ -131,6 +131,8 @@ def _load() -> ctypes.CDLL:
         "pb_random_playout": (ctypes.c_int, [P(ctypes.c_uint64), ctypes.c_int, P(Pos)]),
         "pb_random_playouts": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(Pos),
                                                P(ctypes.c_int)]),
+        "pb_u128_add": (None, [P(U128), P(U128)]),
+        "pb_u128_text": (ctypes.c_int, [P(U128), ctypes.c_char_p, ctypes.c_size_t]),
         "pb_device_count": (ctypes.c_int, []),
         "pb_choose_launch_depth": (ctypes.c_int, [ctypes.c_void_p, P(Pos)]),
         "pb_prepare": (ctypes.c_int, [ctypes.c_void_p, P(Pos), ctypes.c_int]),
@@ -234,6 +236,25 @@ def hash_after_move(key: int, p: Pos, move: int) -> int:
     out = U128()
     lib.pb_hash_after_move(ctypes.byref(k), ctypes.byref(p), move, ctypes.byref(out))
     return out.value()
+
+
+def u128_add(acc: int, v: int) -> int:
+    """acc + v through the library's 128-bit accumulation (the one the host
+    recursion applies to subtree counts), wrapping at 2^128 like the C type."""
+    a = U128(acc & ((1 << 64) - 1), (acc >> 64) & ((1 << 64) - 1))
+    b = U128(v & ((1 << 64) - 1), (v >> 64) & ((1 << 64) - 1))
+    lib.pb_u128_add(ctypes.byref(a), ctypes.byref(b))
+    return a.value()
+
+
+def u128_text(v: int) -> str:
+    """Decimal text of a 128-bit count as the command line prints it."""
+    x = U128(v & ((1 << 64) - 1), (v >> 64) & ((1 << 64) - 1))
+    buf = ctypes.create_string_buffer(48)
+    n = lib.pb_u128_text(ctypes.byref(x), buf, 48)
+    if n < 0:
+        raise PerftError(n, "u128 text")
+    return buf.value.decode()
 
 
 def move_uci(m: int) -> str:

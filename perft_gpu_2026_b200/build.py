@@ -1,7 +1,9 @@
 """Build recipe for the native parts of perft_gpu_2026_b200.
 
     python -m perft_gpu_2026_b200.build            # library + CLI
-    python -m perft_gpu_2026_b200.build --oracle   # also the test oracle
+    python -m perft_gpu_2026_b200.build --oracle   # also the test oracle (and the
+                                                   # reference binary when
+                                                   # PERFT_REFERENCE_DIR is set)
 
 Outputs (in-tree, git-ignored, shipped with the repository snapshot):
   perft_gpu_2026_b200/libperftb200.so   CUDA kernels for sm_100a + host driver + C ABI
@@ -59,20 +61,21 @@ def build_cli(force: bool = False) -> str:
     return CLI
 
 
-def build_oracle(with_reference: bool = True) -> None:
-    """The checker: oracle/liboracle.so, and oracle/_ref/perft_gpu_ref when the
-    reference sources are present on this machine."""
+def build_oracle(reference_dir: str | None = None) -> None:
+    """The checker: oracle/liboracle.so, and oracle/_ref/perft_gpu_ref when a
+    directory holding the reference sources is given (argument, else the
+    PERFT_REFERENCE_DIR environment variable)."""
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
-    ref = os.environ.get("PERFT_REFERENCE_DIR", "/root/reference")
-    if with_reference and os.path.isdir(ref):
+    ref = reference_dir or os.environ.get("PERFT_REFERENCE_DIR")
+    if ref and os.path.isdir(ref):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref], check=True)
 
 
-def build_all(force: bool = False, oracle: bool = True) -> None:
+def build_all(force: bool = False, oracle: bool = True, reference_dir: str | None = None) -> None:
     build_library(force)
     build_cli(force)
     if oracle:
-        build_oracle()
+        build_oracle(reference_dir)
 
 
 if __name__ == "__main__":

@@ -8,7 +8,7 @@
 // splitmix64 stream (seed fixed below), so the output is reproducible.
 //
 // Build and run (writes to stdout):
-//   g++ -O2 -o /tmp/magic_search magic_search.cpp && /tmp/magic_search > magic_numbers.inc
+//   g++ -O2 -o magic_search magic_search.cpp && ./magic_search > magic_numbers.inc
 #include <cstdint>
 #include <cstdio>
 #include <vector>

@@ -18,7 +18,6 @@
 #include <algorithm>
 #include <chrono>
 #include <string>
-#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -1289,6 +1288,28 @@ inline void add128(pb_u128 &a, const pb_u128 &b)
     a.hi += b.hi + (a.lo < old ? 1 : 0);
 }
 
+// Decimal text of a 128-bit value: repeated division of four 32-bit limbs by
+// 10^9, nine digits per step, most significant group unpadded.
+int u128_decimal(pb_u128 v, char *buf, size_t len)
+{
+    if (!buf || len < 40) return PB_ERR_ARG;  // 2^128 - 1 has 39 digits
+    uint32_t limb[4] = {(uint32_t)v.lo, (uint32_t)(v.lo >> 32), (uint32_t)v.hi, (uint32_t)(v.hi >> 32)};
+    uint32_t groups[5];
+    int ng = 0;
+    do {
+        u64 rem = 0;
+        for (int i = 3; i >= 0; i--) {
+            u64 cur = (rem << 32) | limb[i];
+            limb[i] = (uint32_t)(cur / 1000000000ULL);
+            rem = cur % 1000000000ULL;
+        }
+        groups[ng++] = (uint32_t)rem;
+    } while (limb[0] | limb[1] | limb[2] | limb[3]);
+    int k = snprintf(buf, len, "%u", groups[ng - 1]);
+    for (int i = ng - 2; i >= 0; i--) k += snprintf(buf + k, len - k, "%09u", groups[i]);
+    return k;
+}
+
 // Host recursion above the launch depth (perft_cpu_recurse, launcher.cu:572-715).
 int launch_recurse(pb_ctx *ctx, const Board &b, u32 st, int c, int depth, const Hash128 &h, pb_u128 *out)
 {
@@ -1355,17 +1376,12 @@ int estimate_launch_depth(pb_ctx *ctx, const Board &b, u32 st, int c)
 // Scratch of pb_scan_u32_noalloc: the scan's tile status words, its tile
 // ticket and its error word live in this fixed device array instead of memory
 // the caller or the engine allocates.  Every GPU that loads the library holds
-// it (34 KB) until the process exits.
-constexpr u64 NOALLOC_SCAN_TILES = 4096;                              // status words
-constexpr u64 NOALLOC_SCAN_MAX_ITEMS = 8388608;                      // counts per call
-static_assert((NOALLOC_SCAN_MAX_ITEMS + SCAN_TILE - 1) / SCAN_TILE <= NOALLOC_SCAN_TILES,
-              "the status words of the largest allowed scan must fit the fixed array");
+// it (8.25 KB: 1,024 status words and 32 spare words) until the process exits.
+constexpr u64 NOALLOC_SCAN_MAX_ITEMS = 8388608;                       // counts per call
+constexpr u64 NOALLOC_SCAN_TILES = NOALLOC_SCAN_MAX_ITEMS / SCAN_TILE;  // status words
+static_assert(NOALLOC_SCAN_TILES * SCAN_TILE == NOALLOC_SCAN_MAX_ITEMS,
+              "the status words cover exactly the largest allowed scan");
 static __device__ __align__(256) u64 g_noalloc_scratch[NOALLOC_SCAN_TILES + 32];
-
-// Device address of g_noalloc_scratch per device, resolved once per device
-// (with that device current) on the first call there.
-static u64 *g_noalloc_addr[64];
-static std::mutex g_noalloc_mu;
 
 // ==================================================================== C ABI
 extern "C" {
@@ -1526,6 +1542,17 @@ int pb_make_move(pb_pos *pos, uint16_t move)
     host_make(b, st, pos->color, move);
     to_pos(b, st, 1 - pos->color, *pos);
     return PB_OK;
+}
+
+void pb_u128_add(pb_u128 *acc, const pb_u128 *v)
+{
+    if (acc && v) add128(*acc, *v);
+}
+
+int pb_u128_text(const pb_u128 *v, char *buf, size_t len)
+{
+    if (!v) return PB_ERR_ARG;
+    return u128_decimal(*v, buf, len);
 }
 
 int pb_perft_cpu(pb_ctx *ctx, const pb_pos *pos, int depth, uint64_t *count)
@@ -1880,20 +1907,19 @@ int pb_scan_u32_noalloc(const uint32_t *d_in, uint64_t n, uint64_t *d_out, uint6
     if (!d_in || !d_out || !d_total) return PB_ERR_ARG;
     if (n > NOALLOC_SCAN_MAX_ITEMS) return PB_ERR_ARG;  // beyond the fixed scratch
     if (n == 0) return PB_OK;
-    build_host_tables();
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PB_ERR_CUDA;
-    u64 *scratch;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
-            void *addr = nullptr;
-            if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return PB_ERR_CUDA;
-            g_noalloc_addr[dev] = reinterpret_cast<u64 *>(addr);
-        }
-        scratch = g_noalloc_addr[dev];
-    }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    // the call waits for its stream, which a capture cannot record
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return PB_ERR_CUDA;
+    if (cap != cudaStreamCaptureStatusNone) return PB_ERR_ARG;
+    build_host_tables();
+    // The device address of the array, looked up on every call with the
+    // caller's device current: the lookup allocates nothing, and a context
+    // reset (which reloads the module and may move the array) cannot leave a
+    // stale address behind.  The first call on a device loads the module.
+    void *addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return PB_ERR_CUDA;
+    u64 *scratch = reinterpret_cast<u64 *>(addr);
     const u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     u64 *status = scratch;
     u32 *ticket = reinterpret_cast<u32 *>(scratch + NOALLOC_SCAN_TILES);

@@ -32,28 +32,13 @@
 #include "../../include/perft_b200.h"
 
 
-// Decimal text of a 128-bit value by repeated division by 10^9 in 32-bit limbs.
+// Decimal text of a 128-bit count (the library's formatter, the reference's
+// uint128::toDecimalString).
 static std::string u128_text(pb_u128 v)
 {
-    if (v.hi == 0) return std::to_string((unsigned long long)v.lo);
-    uint32_t limb[4] = {(uint32_t)v.lo, (uint32_t)(v.lo >> 32), (uint32_t)v.hi, (uint32_t)(v.hi >> 32)};
-    std::vector<uint32_t> groups;
-    while (limb[0] | limb[1] | limb[2] | limb[3]) {
-        uint64_t rem = 0;
-        for (int i = 3; i >= 0; i--) {
-            uint64_t cur = (rem << 32) | limb[i];
-            limb[i] = (uint32_t)(cur / 1000000000ULL);
-            rem = cur % 1000000000ULL;
-        }
-        groups.push_back((uint32_t)rem);
-    }
-    std::string s = std::to_string(groups.back());
-    char buf[16];
-    for (int i = (int)groups.size() - 2; i >= 0; i--) {
-        snprintf(buf, sizeof(buf), "%09u", groups[i]);
-        s += buf;
-    }
-    return s;
+    char buf[48];
+    pb_u128_text(&v, buf, sizeof(buf));
+    return buf;
 }
 
 static double u128_double(pb_u128 v) { return (double)v.hi * 18446744073709551616.0 + (double)v.lo; }
@@ -141,9 +126,8 @@ static int run_batch(const std::string &path, int depth_arg, bool cpu, bool json
         }
         pb_u128 total{0, 0};
         for (int i = 0; i < n; i++) {
-            unsigned long long old = total.lo;
-            total.lo += counts[i];
-            if (total.lo < old) total.hi++;
+            pb_u128 c{counts[i], 0};
+            pb_u128_add(&total, &c);
             const char *mark = "";
             for (auto &e : lines[i].expect)
                 if (e.first == d && e.second != counts[i]) {
@@ -177,9 +161,9 @@ static std::string move_text(uint16_t m)
 
 static pb_u128 add_u128(pb_u128 a, uint64_t b)
 {
-    pb_u128 r{a.lo + b, a.hi};
-    if (r.lo < a.lo) r.hi++;
-    return r;
+    pb_u128 c{b, 0};
+    pb_u128_add(&a, &c);
+    return a;
 }
 
 // The final depth, one root move at a time, with the journal file: lines

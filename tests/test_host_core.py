@@ -225,3 +225,32 @@ def test_cli_journal_resumes_a_partial_run(tmp_path):
     lines, out = run()
     assert lines == want and "journal: 20 root moves read back" in out
     assert len([r for r in j.read_text().splitlines() if r.startswith("4 ")]) == 48
+
+
+def test_u128_accumulation_and_text_across_2_64():
+    """128-bit counts (uint128.h:46-108): the library's accumulation, the one
+    the host recursion applies to every subtree count, carries into the high
+    word, and the printed text is the exact decimal value.  The reference's
+    start position perft 14 total (README.md:63) is the known value past 2^64."""
+    import random
+
+    two64 = 1 << 64
+    rng = random.Random(5)
+    # subtree counts near 2^63..2^64: the running sum crosses 2^64 many times
+    vals = [rng.randrange(two64 // 2, two64) for _ in range(200)] + [two64 - 1, 1, 0, two64 - 1]
+    acc = 0
+    for v in vals:
+        acc = pg.u128_add(acc, v)
+    assert acc == sum(vals) and acc >> 64 > 1
+    assert pg.u128_add(two64 - 1, 1) == two64  # carry out of the low word
+    perft14 = 61885021521585529237
+    assert perft14 > two64
+    for v in (0, 1, 999_999_999, 1_000_000_000, two64 - 1, two64, two64 + 1, perft14, acc,
+              10 ** 27, 10 ** 27 - 1, (1 << 128) - 1):
+        assert pg.u128_text(v) == str(v), v
+    # the sum of the perft 14 total split into u64-sized parts
+    parts = [perft14 // 7] * 6 + [perft14 - 6 * (perft14 // 7)]
+    acc = 0
+    for v in parts:
+        acc = pg.u128_add(acc, v)
+    assert pg.u128_text(acc) == "61885021521585529237"

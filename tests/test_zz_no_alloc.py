@@ -53,6 +53,61 @@ def test_noalloc_scan_matches_regular_entry_point():
     eng.close()
 
 
+def test_noalloc_scan_unaligned_buffers_on_a_side_stream():
+    """Caller buffers off the 32-byte boundary take the scan's scalar path;
+    the call runs on a caller-created stream, twice in a row."""
+    import torch
+
+    torch.cuda.set_device(0)
+    fn = _noalloc()
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=64 << 20)
+    g = torch.Generator().manual_seed(99)
+    side = torch.cuda.Stream()
+    for n in (1_000_003, 70_001):
+        x = torch.randint(0, 219, (n,), generator=g, dtype=torch.int64)
+        buf_in = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+        buf_in[1:].copy_(x.to(torch.int32))
+        out_a = torch.full((n + 1,), -1, dtype=torch.int64, device="cuda")
+        tot_a = torch.full((2,), -1, dtype=torch.int64, device="cuda")
+        out_b = torch.full((n,), -2, dtype=torch.int64, device="cuda")
+        tot_b = torch.full((1,), -2, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        # one element in: 4 bytes off for the counts, 8 for the offsets
+        rc = fn(buf_in.data_ptr() + 4, n, out_a.data_ptr() + 8, tot_a.data_ptr() + 8, side.cuda_stream)
+        assert rc == pg.PB_OK
+        eng.dev_scan(buf_in.data_ptr() + 4, n, out_b.data_ptr(), tot_b.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.equal(out_a[1:], out_b)
+        assert int(tot_a[1].item()) == int(tot_b.item()) == int(x.sum())
+        assert torch.equal(out_b, torch.cumsum(x, 0).cuda() - x.cuda())
+        assert int(out_a[0].item()) == -1 and int(tot_a[0].item()) == -1  # nothing written before the buffers
+    eng.close()
+
+
+def test_noalloc_scan_refuses_a_capturing_stream():
+    """The call waits for its stream, which a CUDA graph capture cannot hold:
+    on a capturing stream it returns PB_ERR_ARG before any GPU work."""
+    import torch
+
+    fn = _noalloc()
+    d = torch.zeros(16, dtype=torch.int32, device="cuda")
+    o = torch.zeros(16, dtype=torch.int64, device="cuda")
+    t = torch.zeros(1, dtype=torch.int64, device="cuda")
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    rcs = []
+    with torch.cuda.stream(s):
+        graph.capture_begin(capture_error_mode="thread_local")
+        try:
+            rcs.append(fn(d.data_ptr(), 16, o.data_ptr(), t.data_ptr(), s.cuda_stream))
+            o.add_(0)  # keep the captured graph non-empty
+        finally:
+            graph.capture_end()
+    assert rcs == [pg.PB_ERR_ARG]
+    del graph
+
+
 def test_noalloc_scan_rejects_sizes_beyond_its_scratch():
     import torch
 
