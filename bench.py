@@ -17,12 +17,21 @@ Printed JSON line (rank 0):
            region (host wall clock around the synchronous call)
   roofline the leaf kernel against the integer-issue roofline
   cpu_baseline  the reference's own -cpu path (oracle/_ref) on this host's
-           cores, one process per core over a sample of depth-2 subtrees
+           cores, one process per core over the root's children (perft 6
+           each), plus a single-process figure and the CPU model
+  reference_gpu  the reference's own GPU build (oracle/_ref, sm_100a) on the
+           same position and depth, one GPU call (launch depth 7), timed by
+           the reference program itself
   positions  (one GPU) positions/s on 4096 uneven roots at perft 5: plain
            per-root calls, count-then-allocate batch, learned planner
+`config` is the same dict in both arms (--impl engine and reference).
 With --gpus N > 1 (torchrun, one process per GPU) the depth-2 subtrees of the
 root are bin-packed over the ranks by their perft(2) (strong scaling: total
-work fixed); the only exchange is one all-reduce of the per-rank counts.
+work fixed); the only exchange is one all-gather of the per-rank counts.
+
+The reference arm (--impl reference) runs only the reference program built
+from its sources: it reads the children's FENs from tests/golden/
+bench_subtrees.json and loads nothing of this repository's library.
 """
 from __future__ import annotations
 
@@ -34,13 +43,53 @@ import subprocess
 import sys
 import tempfile
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = {"workload": "single-position perft", "position": "4 random plies from the initial array, splitmix64 seed 1",
-            "depth": 7, "tt": False}
 METRIC = "leaf nodes/s"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "perft_gpu_ref")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+DEPTH = 7
+
+
+def _bench_position():
+    """(root FEN, its children's FENs) from the committed fixture."""
+    with open(os.path.join(GOLDEN, "bench_subtrees.json")) as f:
+        d = json.load(f)
+    return d["root_fen"], d["children"]
+
+
+def _reference_counts():
+    """The reference's own per-depth counts of the bench position (1..7)."""
+    path = os.path.join(GOLDEN, "ref_configs.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)["config2"]["counts"]
+
+
+def bench_config(depth: int):
+    """The workload description both arms print verbatim."""
+    fen, _ = _bench_position()
+    ref = _reference_counts()
+    return {"workload": "single-position perft", "position": "4 random plies from the initial array, splitmix64 seed 1",
+            "fen": fen, "depth": depth, "tt": False,
+            "nodes": ref[depth - 1] if ref and depth <= len(ref) else None,
+            "l2": "GPU arm: L2 flushed by a 256 MB write before each timed step",
+            "parallelism": "one root; with N ranks its depth-2 subtrees bin-packed by perft(2)"}
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 # leaf kernel launched for each pb_tuning.leaf_kernel value
@@ -131,47 +180,68 @@ def flush_l2(torch, dev):
     del buf
 
 
-def depth2_subtrees(pg, root):
-    """The root's grandchildren (positions two plies down) in generation order."""
-    out = []
-    for m in pg.generate_moves(root):
-        c = pg.make_move(root, m)
-        for m2 in pg.generate_moves(c):
-            out.append(pg.make_move(c, m2))
+def cpu_reference_sample(subtrees, sub_depth, max_seconds=20.0, procs=None):
+    """The reference's -cpu -nott path on this host: `procs` processes kept
+    busy over the subtrees in order (perft sub_depth of each); no subtree is
+    started once the sample budget is spent, those started run to the end.
+    Returns None when the reference is not built."""
+    if not os.path.exists(REF_BIN):
+        return None
+    procs = procs or len(os.sched_getaffinity(0))
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    t0 = time.perf_counter()
+
+    def one(fen):
+        if time.perf_counter() - t0 >= max_seconds:
+            return None
+        out = subprocess.run([REF_BIN, fen, str(sub_depth), "-cpu", "-nott"], capture_output=True, text=True,
+                             env=env).stdout
+        last = [l for l in out.splitlines() if l.startswith(f"Perft({sub_depth:02d})")]
+        return int(last[0].split(":")[1].split(",")[0]) if last else None
+
+    with ThreadPoolExecutor(max_workers=procs) as ex:
+        res = list(ex.map(one, subtrees))
+    wall = time.perf_counter() - t0
+    done = [r for r in res if r is not None]
+    nodes = sum(done)
+    return {"value": nodes / wall if wall > 0 else 0.0, "unit": METRIC, "cores": procs, "kind": "reference",
+            "sample": f"{len(done)} of the bench position's {len(subtrees)} children at perft {sub_depth} "
+                      f"(reference -cpu -nott, one process per child, {procs} at a time, {wall:.1f} s wall)",
+            "nodes": nodes, "seconds": wall}
+
+
+def cpu_baseline(children, depth, all_core_s=15.0, single_s=8.0):
+    """All host cores (one reference process per core) and one process."""
+    allc = cpu_reference_sample(children, depth - 1, max_seconds=all_core_s)
+    if allc is None:
+        return None
+    one = cpu_reference_sample(children, depth - 1, max_seconds=single_s, procs=1)
+    out = {k: allc[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    out["single_thread"] = {"value": one["value"], "unit": METRIC, "sample": one["sample"]}
+    out["cpu_model"] = cpu_model()
+    out["host_threads"] = os.cpu_count()
     return out
 
 
-def cpu_reference_sample(pg, root, depth, max_seconds=20.0, cores=None):
-    """The reference's -cpu path on this host: one process per core, each on a
-    depth-2 subtree (perft depth-2 of a grandchild), until the sample budget."""
-    ref = os.path.join(ROOT, "oracle", "_ref", "perft_gpu_ref")
-    kind = "reference"
-    if not os.path.exists(ref):
+def reference_gpu(fen, depth, reps=3):
+    """The reference's own GPU build on the bench position: perft `depth`
+    without tables at launch depth `depth` (one GPU call), the depth line's
+    time as the reference program prints it.  Best of `reps` runs."""
+    if not os.path.exists(REF_BIN):
         return None
-    cores = cores or len(os.sched_getaffinity(0))
-    subs = depth2_subtrees(pg, root)
-    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
-    sub_depth = depth - 2
-    nodes, done = 0, 0
-    t0 = time.perf_counter()
-    i = 0
-    # waves of `cores` processes until the budget is spent
-    while i < len(subs) and time.perf_counter() - t0 < max_seconds:
-        wave = subs[i:i + cores]
-        procs = [subprocess.Popen([ref, pg.to_fen(s), str(sub_depth), "-cpu", "-nott"], stdout=subprocess.PIPE,
-                                  stderr=subprocess.DEVNULL, text=True, env=env) for s in wave]
-        for pr in procs:
-            out, _ = pr.communicate()
-            last = [l for l in out.splitlines() if l.startswith(f"Perft({sub_depth:02d})")]
-            if last:
-                nodes += int(last[0].split(":")[1].split(",")[0])
-                done += 1
-        i += cores
-    wall = time.perf_counter() - t0
-    return {"value": nodes / wall if wall > 0 else 0.0, "unit": METRIC, "cores": cores, "kind": kind,
-            "sample": f"{done} of {len(subs)} depth-2 subtrees of the bench position at perft {sub_depth} "
-                      f"(reference -cpu -nott, {cores} processes in parallel, {wall:.1f} s wall)",
-            "nodes": nodes, "seconds": wall}
+    times, nodes = [], None
+    for _ in range(reps):
+        out = subprocess.run([REF_BIN, fen, str(depth), "-nott", "-ld", str(depth)], capture_output=True, text=True,
+                             timeout=600).stdout
+        line = [l for l in out.splitlines() if l.startswith(f"Perft({depth:02d})")]
+        if not line:
+            return {"unavailable": "reference GPU build printed no depth line"}
+        nodes = int(line[0].split(":")[1].split(",")[0])
+        times.append(float(line[0].split("time:")[1].split("seconds")[0]))
+    best = min(times)
+    return {"value": nodes / best, "unit": METRIC, "nodes": nodes, "seconds": times,
+            "source": f"oracle/_ref/perft_gpu_ref <fen> {depth} -nott -ld {depth} (reference sources built for "
+                      "sm_100a), the time it prints for the depth line, best of the runs"}
 
 
 def positions_section(pg, eng, reps):
@@ -221,21 +291,18 @@ def positions_section(pg, eng, reps):
 
 
 def run_reference_arm(args):
-    import perft_gpu_2026_b200 as pg
-
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    root = pg.config_position(4, 1)
-    vals = []
-    last = None
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/perft_gpu_ref not built"}))
+        return 0
+    _, subs = _bench_position()
+    vals, last = [], None
     # each step is a bounded sample; the whole run stays near two minutes
     per_step = max(1.0, min(8.0, 120.0 / (args.warmup + args.steps)))
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_sample(pg, root, WORKLOAD["depth"], max_seconds=per_step)
-        if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/perft_gpu_ref not built"}))
-            return 0
+        r = cpu_reference_sample(subs, args.depth - 1, max_seconds=per_step)
         if i >= args.warmup:
             vals.append(r["value"])
             last = r
@@ -243,9 +310,9 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": last["seconds"] * 1e3,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": WORKLOAD,
+            "config": bench_config(args.depth),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": last["cores"], "kind": "reference",
-                             "sample": last["sample"]},
+                             "sample": last["sample"], "cpu_model": cpu_model(), "host_threads": os.cpu_count()},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -257,11 +324,12 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--depth", type=int, default=WORKLOAD["depth"])
+    ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--leaf-kernel", type=int, default=0, help="1 = edge per thread, 2 = cooperative (0 = engine default)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default launch parameters")
     ap.add_argument("--no-positions", action="store_true", help="skip the batched-roots positions/s section")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's GPU build")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -283,7 +351,8 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
 
-    root = pg.config_position(4, 1)
+    root_fen, child_fens = _bench_position()
+    root = pg.parse_fen(root_fen)
     depth = args.depth
     eng = pg.Engine(device=local, use_tt=False)
     tuning = None
@@ -306,17 +375,11 @@ def main():
     from perft_gpu_2026_b200 import dist as pdist
 
     if world > 1:
-        subs = pdist.subtrees(root, 2)
-        mine = pdist.shard_balanced(subs, eng.perft_batch(subs, [2] * len(subs)), world, rank)
-        sub_depth = depth - 2
+        plan = pdist.ShardedPerft(root, depth, world, rank, lambda ps, d: eng.perft_batch(ps, [d] * len(ps)))
+        run_once = plan.run
     else:
-        mine = [root]
-        sub_depth = depth
-
-    def run_once():
-        if len(mine) == 1:
-            return eng.perft_position(mine[0], sub_depth)
-        return sum(eng.perft_batch(mine, [sub_depth] * len(mine)))
+        def run_once():
+            return eng.perft_position(root, depth)
 
     def step():
         total = run_once()
@@ -359,9 +422,10 @@ def main():
         t = torch.tensor([my_ms, my_e2e, my_leaf_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         my_ms, my_e2e, my_leaf_ms = t.tolist()
-        c = torch.tensor([nodes], dtype=torch.int64, device=dev)
-        dist.all_reduce(c)
-        nodes = int(c.item())
+        nodes = pdist.all_reduce_count(nodes, device=dev)
+    config = bench_config(depth)
+    if config["nodes"] is not None and nodes != config["nodes"]:
+        raise SystemExit(f"count {nodes} differs from the reference's {config['nodes']}")
     if rank == 0:
         peaks, peak_kind = _peaks()
         kernel = LEAF_KERNELS.get(eng.get_tuning().leaf_kernel, "k_leaf2")
@@ -394,9 +458,9 @@ def main():
         line = {"metric": METRIC, "value": nodes / (my_ms / 1e3), "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": my_ms, "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-                "config": dict(WORKLOAD, depth=depth, nodes=nodes, l2="flushed (256 MB write) before each step",
-                               parallelism=f"depth-2 subtrees over {world} rank(s)",
-                               tuning=eng.get_tuning().as_dict()),
+                "config": config, "tuning": eng.get_tuning().as_dict(),
+                "count_check": "equal to the reference program's count of this position and depth"
+                               if config["nodes"] is not None else "no reference count for this depth",
                 "e2e": {"value": nodes / (my_e2e / 1e3), "unit": METRIC, "ms_per_step": my_e2e,
                         "h2d_bytes_per_step": int(results[0][5]), "d2h_bytes_per_step": int(results[0][6]),
                         "timing": "host wall clock around pb_perft_position"},
@@ -404,11 +468,17 @@ def main():
         if world == 1 and not args.no_positions:
             line["positions"] = positions_section(pg, eng, reps=min(args.steps, 3))
         if world == 1 and not args.no_cpu_baseline:
-            cb = cpu_reference_sample(pg, root, depth, max_seconds=15.0)
+            cb = cpu_baseline(child_fens, depth)
             if cb:
-                line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        print(json.dumps(line))
+                line["cpu_baseline"] = cb
     eng.close()
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        # after the engine released its memory; the reference allocates its own
+        rg = reference_gpu(root_fen, depth)
+        if rg:
+            line["reference_gpu"] = rg
+    if rank == 0:
+        print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()

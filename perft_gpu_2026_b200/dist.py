@@ -1,9 +1,9 @@
 """Multi-GPU sharding of one perft: one process per GPU (torch.distributed).
 
 The perft tree splits into independent subtrees, so ranks need no data
-exchange while they count: rank r takes the subtrees r, r+N, r+2N, ... of the
-root's positions `split_plies` plies down, and one all-reduce of the u64
-counts gives the total.  Works with the nccl backend (GPU engines) and the
+exchange while they count: each rank takes a share of the root's positions
+`split_plies` plies down (round robin, or bin-packed by size), and one
+all-gather of the per-rank u64 counts gives the exact total.  Works with the nccl backend (GPU engines) and the
 gloo backend (host engines, used by the CPU tests).
 """
 from __future__ import annotations
@@ -67,10 +67,40 @@ def perft_sharded(root: pg.Pos, depth: int, count: Callable[[List[pg.Pos], int],
 
 
 def all_reduce_count(value: int, device=None) -> int:
-    """Sums a u64 count over the process group (one collective)."""
+    """Sums the ranks' u64 counts exactly (one collective): every rank's count
+    travels as the bit pattern of a 64-bit word (all-gather) and the sum is
+    taken in Python integers, so it is exact past 2^63 and past 2^64 (the
+    128-bit totals the reference prints, uint128.h:13-108)."""
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.int64, device=device)
-    dist.all_reduce(t)
-    return int(t.item())
+    if not 0 <= value < (1 << 64):
+        raise ValueError("a rank's count must fit 64 bits")
+    word = value - (1 << 64) if value >= (1 << 63) else value
+    t = torch.tensor([word], dtype=torch.int64, device=device)
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size())]
+    dist.all_gather(parts, t)
+    return sum(int(x.item()) & ((1 << 64) - 1) for x in parts)
+
+
+class ShardedPerft:
+    """This rank's share of perft(depth) of one root, as bench.py runs it
+    under torchrun: the root's positions `split_plies` plies down are
+    bin-packed over the ranks by their exact perft(2) (balanced_assignment;
+    every rank computes the same split), and run() counts this rank's
+    subtrees at depth - split_plies with count_batch(positions, depth) ->
+    counts (the engine's batched GPU call; a host loop in the CPU tests).
+    all_reduce_count then gives the total."""
+
+    def __init__(self, root: pg.Pos, depth: int, world: int, rank: int,
+                 count_batch: Callable[[List[pg.Pos], int], Sequence[int]], split_plies: int = 2):
+        if depth <= split_plies:
+            raise ValueError("depth must exceed the split depth")
+        self.count_batch = count_batch
+        subs = subtrees(root, split_plies)
+        self.weights = list(count_batch(subs, 2))
+        self.mine = shard_balanced(subs, self.weights, world, rank)
+        self.sub_depth = depth - split_plies
+
+    def run(self) -> int:
+        return int(sum(self.count_batch(self.mine, self.sub_depth))) if self.mine else 0

@@ -41,6 +41,49 @@ def _worker(rank, world, port, fen, depth, balanced, q):
     dist.destroy_process_group()
 
 
+def _bench_worker(rank, world, port, depth, q):
+    """bench.py's multi-rank path: ShardedPerft's split and per-rank count,
+    then the exact u64 reduction (host counting in place of the GPU batch)."""
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    eng = pg.Engine(device=-1)
+    root = pg.config_position(4, 1)
+    plan = pdist.ShardedPerft(root, depth, world, rank, lambda ps, d: [eng.perft_cpu(p, d) for p in ps])
+    part = plan.run()
+    total = pdist.all_reduce_count(part)
+    # counts past 2^63 (a signed 64-bit all-reduce would wrap): each rank
+    # contributes 2^64 - 1 - rank
+    big = pdist.all_reduce_count((1 << 64) - 1 - rank)
+    q.put((rank, part, total, big, len(plan.mine)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_bench_multi_rank_path_on_gloo(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    depth = 4
+    procs = [ctx.Process(target=_bench_worker, args=(r, world, port, depth, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    want = pg.Engine(device=-1).perft_cpu(pg.config_position(4, 1), depth)
+    assert all(total == want for _, _, total, _, _ in res)
+    assert sum(part for _, part, _, _, _ in res) == want
+    assert sum(n for *_, n in res) == len(pdist.subtrees(pg.config_position(4, 1), 2))
+    assert all(big == sum((1 << 64) - 1 - r for r in range(world)) for _, _, _, big, _ in res)
+
+
 @pytest.mark.parametrize("balanced", [False, True])
 @pytest.mark.parametrize("fen,depth", [(pg.START_FEN, 4), ("r3k2r/p1ppqpb1/bn2pnp1/3PN3/1p2P3/2N2Q1p/PPPBBPPP/R3K2R w KQkq -", 3)])
 def test_two_rank_gloo_perft(fen, depth, balanced):

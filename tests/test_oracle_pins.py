@@ -42,3 +42,22 @@ def test_oracle_strict_differs_only_on_merged_moves(oracle):
 def test_oracle_strict_count_equals_generation(oracle, golden):
     for case in golden:
         assert oracle.count(case["fen"], strict=True) == len(oracle.moves(case["fen"])), case["name"]
+
+
+def test_oracle_matches_reference_on_benchmark_workloads(oracle):
+    """tests/golden/ref_configs.json holds the reference's counts on the
+    benchmark workloads; the oracle reproduces the ones it finishes in
+    seconds (configs 1, 2 and 5 to perft 5; config 4's label rows to perft
+    3).  The full depths are compared on the GPU."""
+    import json
+    import os
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_configs.json")
+    with open(path) as f:
+        cfg = json.load(f)
+    for name in ("config1", "config2", "config5"):
+        c = cfg[name]
+        assert [oracle.perft(c["fen"], d) for d in range(1, 6)] == c["counts"][:5], name
+    c = cfg["config4"]
+    for fen, want in zip(c["fens"], c["perft1_4"]):
+        assert [oracle.perft(fen, d) for d in (1, 2, 3)] == want[:3], fen
