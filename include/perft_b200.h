@@ -120,6 +120,15 @@ int pb_perft(pb_ctx *ctx, const char *fen, int max_depth, pb_u128 *per_depth, do
 void pb_u128_add(pb_u128 *acc, const pb_u128 *v);
 int pb_u128_text(const pb_u128 *v, char *buf, size_t len);
 
+/* Self-test of the listed-piece move count (leaf kernel 5), on the host: for
+ * every child of each position, the count with the side's piece squares
+ * listed from the parent position equals the count from the child's piece
+ * bitboards (both counting conventions, in and out of check).  No
+ * counterpart in the reference.  *checked = children compared (positions
+ * with more than four knights, diagonal or orthogonal movers are skipped),
+ * *mismatches = disagreements. */
+int pb_selftest_listed_counts(const pb_pos *pos, int n, uint64_t *checked, uint64_t *mismatches);
+
 /* Replaces perft_cpu_dispatch (launcher.cu:807-816): host-only perft. */
 int pb_perft_cpu(pb_ctx *ctx, const pb_pos *pos, int depth, uint64_t *count);
 
@@ -170,18 +179,23 @@ typedef struct {
  * Zero fields keep the current value.  leaf_kernel: 1 = one edge per thread,
  * 2 = cooperative (grandchildren spread over the CTA), 3 = in-check children
  * deferred to a second pass, 4 = one edge per thread with the CTA's children
- * ranked by move count first (default);
+ * ranked by move count first (default), 5 = as 4 with each child's own-piece
+ * squares listed once for all of its grandchild counts (batched, planned and
+ * table leaves rank their children for 4 and 5);
  * leaf_blocks_per_sm: persistent grid of the cooperative leaf. */
 typedef struct {
     int leaf_kernel;
     int leaf_blocks_per_sm;
-    int leaf_threads;   /* CTA size of leaf kernels 1, 3 and 4: 128, 256 (default) or 512 (not 3) */
+    int leaf_threads;   /* CTA size of leaf kernels 1, 3, 4 and 5: 128, 256 (default) or 512 (not 3) */
     int gen_threads;    /* CTA size of the staged generator: 64 or 128 (default); stages 64 moves per thread */
     int leaf_fuse;      /* plies fused in the leaf kernel: 2 (default) or 1 (one more BFS level) */
     int tt_replace;     /* device TT replacement: 1 = always overwrite (default, tt.h:60-70),
                            2 = two-slot buckets, the larger subtree keeps the first slot;
                            takes effect when the device tables are next sized */
-    int reserved[2];
+    int planned_leaf;   /* leaf of planned (graph-captured) batches: 1 = grid over the planned
+                           capacity, CTAs past the level's size leave at once (default);
+                           2 = persistent CTAs fed by an atomic work queue */
+    int reserved;
 } pb_tuning;
 
 int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t);

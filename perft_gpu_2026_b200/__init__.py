@@ -87,11 +87,11 @@ class Tuning(ctypes.Structure):
 
     _fields_ = [("leaf_kernel", ctypes.c_int), ("leaf_blocks_per_sm", ctypes.c_int),
                 ("leaf_threads", ctypes.c_int), ("gen_threads", ctypes.c_int), ("leaf_fuse", ctypes.c_int),
-                ("tt_replace", ctypes.c_int), ("reserved", ctypes.c_int * 2)]
+                ("tt_replace", ctypes.c_int), ("planned_leaf", ctypes.c_int), ("reserved", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k in ("leaf_kernel", "leaf_blocks_per_sm", "leaf_threads", "gen_threads",
-                                              "leaf_fuse", "tt_replace")}
+                                              "leaf_fuse", "tt_replace", "planned_leaf")}
 
 
 class PlanStats(ctypes.Structure):
@@ -131,6 +131,7 @@ def _load() -> ctypes.CDLL:
         "pb_random_playout": (ctypes.c_int, [P(ctypes.c_uint64), ctypes.c_int, P(Pos)]),
         "pb_random_playouts": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, P(Pos),
                                                P(ctypes.c_int)]),
+        "pb_selftest_listed_counts": (ctypes.c_int, [P(Pos), ctypes.c_int, P(ctypes.c_uint64), P(ctypes.c_uint64)]),
         "pb_u128_add": (None, [P(U128), P(U128)]),
         "pb_u128_text": (ctypes.c_int, [P(U128), ctypes.c_char_p, ctypes.c_size_t]),
         "pb_device_count": (ctypes.c_int, []),
@@ -236,6 +237,17 @@ def hash_after_move(key: int, p: Pos, move: int) -> int:
     out = U128()
     lib.pb_hash_after_move(ctypes.byref(k), ctypes.byref(p), move, ctypes.byref(out))
     return out.value()
+
+
+def selftest_listed_counts(positions: Sequence[Pos]) -> Tuple[int, int]:
+    """(children compared, mismatches) of the listed-piece move count against
+    the bitboard count, on the host, over every child of each position."""
+    arr = (Pos * len(positions))(*positions)
+    checked, bad = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    rc = lib.pb_selftest_listed_counts(arr, len(positions), ctypes.byref(checked), ctypes.byref(bad))
+    if rc != PB_OK:
+        raise PerftError(rc, "listed-count self-test")
+    return checked.value, bad.value
 
 
 def u128_add(acc: int, v: int) -> int:
@@ -416,14 +428,18 @@ class Engine:
         self._check(lib.pb_set_timing(self._h, int(enable)))
 
     def set_tuning(self, leaf_kernel: int = 0, leaf_blocks_per_sm: int = 0, leaf_threads: int = 0,
-                   gen_threads: int = 0, leaf_fuse: int = 0, tt_replace: int = 0) -> None:
+                   gen_threads: int = 0, leaf_fuse: int = 0, tt_replace: int = 0, planned_leaf: int = 0) -> None:
         """Launch parameters (pb_set_tuning); 0 keeps the current value.
         leaf_kernel 1 = one edge per thread, 2 = cooperative, 3 = in-check
-        children deferred, 4 = children ranked by move count (default);
+        children deferred, 4 = children ranked by move count (default),
+        5 = ranked with each child's own-piece squares listed once;
         leaf_threads 128/256/512; gen_threads 64/128; leaf_fuse 1/2;
-        tt_replace 1 = always overwrite, 2 = two-slot size priority."""
+        tt_replace 1 = always overwrite, 2 = two-slot size priority;
+        planned_leaf 1 = grid over the planned capacity (default),
+        2 = persistent work-queue leaf."""
         t = Tuning()
         t.tt_replace = tt_replace
+        t.planned_leaf = planned_leaf
         t.leaf_kernel = leaf_kernel
         t.leaf_blocks_per_sm = leaf_blocks_per_sm
         t.leaf_threads = leaf_threads

@@ -261,6 +261,98 @@ template <int C> PB_HD u64 enemy_attacks(const Sets &s, u64 my_king, int ksq)
     return a;
 }
 
+// ---------------------------------------------------------------- own pieces
+// Moves of the side to move's knights, bishops, rooks and queens, counted for
+// the move counters below: pieces in `movable` (own and not pinned) move to
+// `targets`; pinned own sliders in `pinned_lines` (empty when in check) move
+// along the line through their king to squares without an own piece.
+//
+// BitboardPieces walks the piece sets of the position being counted.
+struct BitboardPieces {
+    PB_HD u32 count(const Sets &s, u64 movable, u64 targets, u64 pinned_lines, int ksq) const
+    {
+        u32 n = 0;
+        for (u64 kn = s.knights & movable; kn; kn &= kn - 1) n += popc(knight_att(lsb(kn)) & targets);
+        for (u64 bs = s.bq & movable; bs; bs &= bs - 1) n += popc(bishop_att(lsb(bs), s.occ) & targets);
+        for (u64 rs = s.rq & movable; rs; rs &= rs - 1) n += popc(rook_att(lsb(rs), s.occ) & targets);
+        if (pinned_lines & (s.bq | s.rq)) {
+            // a pinned slider moves only along the line through its king
+            for (u64 bs = s.bq & s.us & pinned_lines; bs; bs &= bs - 1) {
+                int sq = lsb(bs);
+                n += popc(bishop_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
+            }
+            for (u64 rs = s.rq & s.us & pinned_lines; rs; rs &= rs - 1) {
+                int sq = lsb(rs);
+                n += popc(rook_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
+            }
+        }
+        return n;
+    }
+};
+
+// ListedPieces serves the positions one move of the OTHER side away from a
+// position P (the grandchildren of the fused leaf): the side to move there has
+// the pieces it had in P, less at most one that the other side captured.  Its
+// knight, diagonal-mover (bishop, queen) and orthogonal-mover (rook, queen)
+// squares are listed once from P, four per kind at most, one byte each
+// (square + 1, 0 = end), so the counts iterate the lists instead of scanning
+// bitboards.  Pieces whose move set differs from the plain one (captured, or
+// pinned) are corrected afterwards; that path is rare.
+struct ListedPieces {
+    u32 kn = 0, dg = 0, og = 0;
+    u64 listed = 0;  // squares in the lists
+
+    // Lists side C's pieces of `b`; false if a kind has more than four.
+    template <int C> PB_HD bool build(const Board &b)
+    {
+        Sets s = derive<C>(b);
+        u64 k = s.knights & s.us, d = s.bq & s.us, o = s.rq & s.us;
+        listed = k | d | o;
+        return pack(k, kn) && pack(d, dg) && pack(o, og);
+    }
+    static PB_HD bool pack(u64 set, u32 &out)
+    {
+        out = 0;
+        for (int k = 0; set; k++, set &= set - 1) {
+            if (k == 4) return false;
+            out |= (u32)(lsb(set) + 1) << (8 * k);
+        }
+        return true;
+    }
+    // true if one of the list's bytes equals key (1..64): a zero-byte test of
+    // the list XOR the key repeated in every byte
+    static PB_HD bool has(u32 list, u32 key)
+    {
+        u32 x = list ^ (key * 0x01010101u);
+        return ((x - 0x01010101u) & ~x & 0x80808080u) != 0;
+    }
+    PB_HD u32 count(const Sets &s, u64 movable, u64 targets, u64 pinned_lines, int ksq) const
+    {
+        u32 n = 0;
+        for (u32 l = kn; l; l >>= 8) n += popc(knight_att((int)(l & 255) - 1) & targets);
+        for (u32 l = dg; l; l >>= 8) n += popc(bishop_att((int)(l & 255) - 1, s.occ) & targets);
+        for (u32 l = og; l; l >>= 8) n += popc(rook_att((int)(l & 255) - 1, s.occ) & targets);
+        // listed squares that are not movable: captured (no longer own) or
+        // pinned.  Take back what the lists counted for them and add the
+        // pinned sliders' moves along their lines.
+        for (u64 fix = listed & ~movable; fix; fix &= fix - 1) {
+            const int sq = lsb(fix);
+            const u32 key = (u32)sq + 1;
+            const u64 line = ((pinned_lines & s.us) >> sq) & 1 ? line_through(sq, ksq) : 0;
+            if (has(kn, key)) n -= popc(knight_att(sq) & targets);
+            if (has(dg, key)) {
+                u64 a = bishop_att(sq, s.occ);
+                n += popc(a & ~s.us & line) - popc(a & targets);
+            }
+            if (has(og, key)) {
+                u64 a = rook_att(sq, s.occ);
+                n += popc(a & ~s.us & line) - popc(a & targets);
+            }
+        }
+        return n;
+    }
+};
+
 // ---------------------------------------------------------------- counting
 // Legal-move count when the side to move is in check
 // (countMovesOutOfCheck, MoveGeneratorBitboard.h:1564-1694).
@@ -316,8 +408,8 @@ PB_HD u32 count_evasions(const Sets &s, u32 state, u64 pinned, u64 threat, int k
 
 // Legal-move count when the side to move is not in check (the main part of
 // countMoves, MoveGeneratorBitboard.h:1729-1943).
-template <int C, bool STRICT>
-PB_HD u32 count_quiet(const Sets &s, u32 state, u64 pinned, u64 threat, int ksq)
+template <int C, bool STRICT, class Own = BitboardPieces>
+PB_HD u32 count_quiet(const Sets &s, u32 state, u64 pinned, u64 threat, int ksq, const Own &own = Own())
 {
     const u64 er = s.rq & s.them;
     u32 n = 0;
@@ -385,25 +477,7 @@ PB_HD u32 count_quiet(const Sets &s, u32 state, u64 pinned, u64 threat, int ksq)
     }
 
     n += popc(king_att(ksq) & ~(threat | s.us));
-
-    u64 kn = s.knights & s.us & ~pinned;
-    while (kn) {
-        n += popc(knight_att(lsb(kn)) & ~s.us);
-        kn &= kn - 1;
-    }
-    for (u64 bs = s.bq & s.us & ~pinned; bs; bs &= bs - 1) n += popc(bishop_att(lsb(bs), s.occ) & ~s.us);
-    for (u64 rs = s.rq & s.us & ~pinned; rs; rs &= rs - 1) n += popc(rook_att(lsb(rs), s.occ) & ~s.us);
-    if (pinned & (s.bq | s.rq)) {
-        // a pinned slider moves only along the line through its king
-        for (u64 bs = s.bq & s.us & pinned; bs; bs &= bs - 1) {
-            int sq = lsb(bs);
-            n += popc(bishop_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
-        }
-        for (u64 rs = s.rq & s.us & pinned; rs; rs &= rs - 1) {
-            int sq = lsb(rs);
-            n += popc(rook_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
-        }
-    }
+    n += own.count(s, s.us & ~pinned, ~s.us, pinned, ksq);
     return n;
 }
 
@@ -439,8 +513,8 @@ template <int C> PB_HD bool prep_in_check(const CountPrep &p) { return (p.threat
 // pawns can take it).  Equal to count_quiet / count_evasions.  On the GPU a
 // group of lanes none of which is in check takes count_quiet, which skips
 // the masking.
-template <int C, bool STRICT>
-PB_HD u32 count_moves(const Board &b, u32 state)
+template <int C, bool STRICT, class Own = BitboardPieces>
+PB_HD u32 count_moves(const Board &b, u32 state, const Own &own = Own())
 {
     const CountPrep p = count_prep<C>(b);
     const Sets &s = p.s;
@@ -449,7 +523,7 @@ PB_HD u32 count_moves(const Board &b, u32 state)
     const bool check = (p.threat & king) != 0;
 #ifdef __CUDA_ARCH__
     // no lane of the converged group in check: the leaner not-in-check path
-    if (!__any_sync(__activemask(), check)) return count_quiet<C, STRICT>(s, state, p.pinned, p.threat, ksq);
+    if (!__any_sync(__activemask(), check)) return count_quiet<C, STRICT>(s, state, p.pinned, p.threat, ksq, own);
 #endif
     u64 safe = ~0ULL, checkers = 0;
     if (check) {
@@ -530,25 +604,7 @@ PB_HD u32 count_moves(const Board &b, u32 state)
         if ((castle & 2) && !(QS_EMPTY & s.occ) && !(QS_SAFE & p.threat)) n++;
     }
 
-    const u64 targets = ~s.us & safe;
-    u64 kn = s.knights & movable;
-    while (kn) {
-        n += popc(knight_att(lsb(kn)) & targets);
-        kn &= kn - 1;
-    }
-    for (u64 bs = s.bq & movable; bs; bs &= bs - 1) n += popc(bishop_att(lsb(bs), s.occ) & targets);
-    for (u64 rs = s.rq & movable; rs; rs &= rs - 1) n += popc(rook_att(lsb(rs), s.occ) & targets);
-    if (pinned & (s.bq | s.rq)) {
-        // a pinned slider moves only along the line through its king
-        for (u64 bs = s.bq & s.us & pinned; bs; bs &= bs - 1) {
-            int sq = lsb(bs);
-            n += popc(bishop_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
-        }
-        for (u64 rs = s.rq & s.us & pinned; rs; rs &= rs - 1) {
-            int sq = lsb(rs);
-            n += popc(rook_att(sq, s.occ) & ~s.us & line_through(sq, ksq));
-        }
-    }
+    n += own.count(s, movable, ~s.us & safe, pinned, ksq);
     return n;
 }
 

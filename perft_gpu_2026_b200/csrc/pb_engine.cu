@@ -39,7 +39,8 @@ struct GraphPlan {
     u64 n = 0;
     int depth = 0;
     bool strict = false;
-    bool sort = false;  // leaf ranks each CTA's children by move count
+    bool sort = false;   // leaf ranks each CTA's children by move count
+    bool queue = false;  // persistent work-queue leaf instead of the grid leaf
     std::vector<u64> caps;
     cudaGraphExec_t exec = nullptr;
     // device buffers inside the arena (fixed for the captured graph)
@@ -48,9 +49,9 @@ struct GraphPlan {
     u32 *r0 = nullptr;
     unsigned long long *rc = nullptr;
     u64 *sizes = nullptr;
-    bool same(u64 n_, int d_, bool s_, bool sort_, const std::vector<u64> &c_) const
+    bool same(u64 n_, int d_, bool s_, bool sort_, bool queue_, const std::vector<u64> &c_) const
     {
-        return exec && n == n_ && depth == d_ && strict == s_ && sort == sort_ && caps == c_;
+        return exec && n == n_ && depth == d_ && strict == s_ && sort == sort_ && queue == queue_ && caps == c_;
     }
 };
 
@@ -71,7 +72,7 @@ struct pb_ctx {
     u64 *h_pinned = nullptr;  // pinned host words for readbacks
     int launch_depth = 0;
     bool timing = false;
-    pb_tuning tuning{4, 0, 256, 128, 2, 1, {0, 0}};
+    pb_tuning tuning{4, 0, 256, 128, 2, 1, 1, 0};
     int num_sms = 0;
     uint16_t *spill = nullptr;  // cooperative-leaf spill area (device)
     size_t spill_blocks = 0;
@@ -201,6 +202,15 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
         switch (ctx->tuning.leaf_threads) {
         case 128: k_leaf2_defer<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         default: k_leaf2_defer<C, S, 256><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        }
+        PB_CUDA(cudaGetLastError());
+        return PB_OK;
+    }
+    if (ctx->tuning.leaf_kernel == 5) {
+        switch (ctx->tuning.leaf_threads) {
+        case 128: k_leaf2_listed<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        case 512: k_leaf2_listed<C, S, 512><<<grid_for(n, 512), 512, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        default: k_leaf2_listed<C, S, 256><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         }
         PB_CUDA(cudaGetLastError());
         return PB_OK;
@@ -554,7 +564,7 @@ int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int dep
     if (n > 0) {
         TTView tv = ctx->dtt.at(2);
         unsigned g = grid_for(n, PB_LEAF_THREADS);
-        const bool sort = ctx->tuning.leaf_kernel == 4;
+        const bool sort = ctx->tuning.leaf_kernel >= 4;
 #define PB_TT_LEAF(CC, SS)                                                                                     \
     if (sort)                                                                                                  \
         k_leaf2_tt<CC, SS, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,     \
@@ -818,7 +828,7 @@ int bfs_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth,
             }
         } else {
             unsigned g = grid_for(ne, PB_LEAF_THREADS);
-            const bool sort = ctx->tuning.leaf_kernel == 4;
+            const bool sort = ctx->tuning.leaf_kernel >= 4;
 #define PB_ROOTED_LEAF(CC, SS)                                                                                   \
     if (sort)                                                                                                    \
         k_leaf2_rooted<CC, SS, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, \
@@ -914,12 +924,30 @@ void launch_leaf_queue_t(cudaStream_t s, int sms, const Board *b, const uint8_t 
     k_leaf2_rooted_queue<C, S, SORT><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev,
                                                                       npar_cap, cursor, rc, counter, err);
 }
-template <int C, bool S>
-void launch_leaf_queue(bool sort, cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r,
-                       const u32 *pi, const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev,
-                       u64 npar_cap, unsigned long long *cursor, unsigned long long *rc, unsigned long long *counter,
-                       u32 *err)
+template <int C, bool S, bool SORT>
+void launch_leaf_grid_t(cudaStream_t s, const Board *b, const uint8_t *st, const u32 *r, const u32 *pi,
+                        const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev, u64 npar_cap,
+                        unsigned long long *rc, unsigned long long *counter, u32 *err)
 {
+    unsigned grid = (unsigned)std::max<u64>((cap + PB_LEAF_THREADS - 1) / PB_LEAF_THREADS, 1);
+    k_leaf2_rooted_dev<C, S, SORT><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap,
+                                                                    rc, counter, err);
+}
+// Leaf of a planned batch: the grid leaf over the planned capacity, or the
+// persistent work-queue leaf (queue).
+template <int C, bool S>
+void launch_leaf_queue(bool sort, bool queue, cudaStream_t s, int sms, const Board *b, const uint8_t *st,
+                       const u32 *r, const u32 *pi, const uint16_t *mv, const u64 *n_dev, u64 cap,
+                       const u64 *npar_dev, u64 npar_cap, unsigned long long *cursor, unsigned long long *rc,
+                       unsigned long long *counter, u32 *err)
+{
+    if (!queue) {
+        if (sort)
+            launch_leaf_grid_t<C, S, true>(s, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, rc, counter, err);
+        else
+            launch_leaf_grid_t<C, S, false>(s, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, rc, counter, err);
+        return;
+    }
     if (sort)
         launch_leaf_queue_t<C, S, true>(s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc, counter, err);
     else
@@ -1033,17 +1061,17 @@ int capture_batch_graph(pb_ctx *ctx, GraphPlan &g)
                                                                 npar_cap, g.rc, ctx->d_err);
     } else if (c == WHITE) {
         if (g.strict)
-            launch_leaf_queue<WHITE, true>(g.sort, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
+            launch_leaf_queue<WHITE, true>(g.sort, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
                                            npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
         else
-            launch_leaf_queue<WHITE, false>(g.sort, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
+            launch_leaf_queue<WHITE, false>(g.sort, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
                                             npar, npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
     } else {
         if (g.strict)
-            launch_leaf_queue<BLACK, true>(g.sort, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
+            launch_leaf_queue<BLACK, true>(g.sort, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
                                            npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
         else
-            launch_leaf_queue<BLACK, false>(g.sort, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
+            launch_leaf_queue<BLACK, false>(g.sort, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
                                             npar, npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -1064,12 +1092,14 @@ int run_planned_batch(pb_ctx *ctx, GraphPlan &g, const Board *rb, const uint8_t 
     NvtxRange nvtx_pass("planned_batch");
     *overflow = false;
     const bool strict = ctx->opts.strict != 0;
-    const bool sort = ctx->tuning.leaf_kernel == 4;
-    if (!g.same(n, depth, strict, sort, caps)) {
+    const bool sort = ctx->tuning.leaf_kernel >= 4;
+    const bool queue = ctx->tuning.planned_leaf == 2;
+    if (!g.same(n, depth, strict, sort, queue, caps)) {
         g.n = n;
         g.depth = depth;
         g.strict = strict;
         g.sort = sort;
+        g.queue = queue;
         g.caps = caps;
         int rc = capture_batch_graph(ctx, g);
         if (rc != PB_OK) {
@@ -1348,6 +1378,41 @@ int launch_recurse(pb_ctx *ctx, const Board &b, u32 st, int c, int depth, const 
     return PB_OK;
 }
 
+// Listed-piece counting against the bitboard counter on every child of
+// `y` (side Z to move): the lists of side 1-Z are taken from y, as the fused
+// leaf takes them from its child position.  Compares both counters (reference
+// and strict conventions) and, for children not in check, the not-in-check
+// counter; returns the number of disagreements, *checked the children compared
+// (0 when a kind has more than four pieces).
+template <int Z>
+u64 check_listed_t(const Board &y, u32 ys, u64 *checked)
+{
+    constexpr int C = 1 - Z;
+    ListedPieces own;
+    *checked = 0;
+    if (!own.build<C>(y)) return 0;
+    uint16_t mv[MAX_MOVES];
+    ArraySink sink{mv, 0};
+    gen_moves<Z>(y, ys, sink);
+    u64 bad = 0;
+    for (int k = 0; k < sink.n; k++) {
+        Board g = y;
+        u32 gs = ys;
+        make_move<Z>(g, gs, mv[k]);
+        bad += count_moves<C, false>(g, gs) != count_moves<C, false>(g, gs, own);
+        bad += count_moves<C, true>(g, gs) != count_moves<C, true>(g, gs, own);
+        const CountPrep p = count_prep<C>(g);
+        if (!prep_in_check<C>(p)) {
+            bad += count_quiet<C, false>(p.s, gs, p.pinned, p.threat, p.ksq) !=
+                   count_quiet<C, false>(p.s, gs, p.pinned, p.threat, p.ksq, own);
+            bad += count_quiet<C, true>(p.s, gs, p.pinned, p.threat, p.ksq) !=
+                   count_quiet<C, true>(p.s, gs, p.pinned, p.threat, p.ksq, own);
+        }
+        ++*checked;
+    }
+    return bad;
+}
+
 // Launch depth: the deepest GPU call whose BFS levels fit half the arena,
 // from the root's branching factor (estimateLaunchDepth, launcher.cu:533-562).
 int estimate_launch_depth(pb_ctx *ctx, const Board &b, u32 st, int c)
@@ -1555,6 +1620,22 @@ int pb_u128_text(const pb_u128 *v, char *buf, size_t len)
     return u128_decimal(*v, buf, len);
 }
 
+int pb_selftest_listed_counts(const pb_pos *pos, int n, uint64_t *checked, uint64_t *mismatches)
+{
+    if (!pos || n < 0 || !checked || !mismatches) return PB_ERR_ARG;
+    build_host_tables();
+    *checked = 0;
+    *mismatches = 0;
+    for (int i = 0; i < n; i++) {
+        u64 c = 0;
+        Board y = to_board(pos[i]);
+        *mismatches += pos[i].color == WHITE ? check_listed_t<WHITE>(y, pos[i].state, &c)
+                                             : check_listed_t<BLACK>(y, pos[i].state, &c);
+        *checked += c;
+    }
+    return PB_OK;
+}
+
 int pb_perft_cpu(pb_ctx *ctx, const pb_pos *pos, int depth, uint64_t *count)
 {
     if (!pos || !count || depth < 0) return PB_ERR_ARG;
@@ -1589,7 +1670,7 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
 {
     if (!ctx || !t) return PB_ERR_ARG;
     if (t->leaf_kernel) {
-        if (t->leaf_kernel < 1 || t->leaf_kernel > 4) return PB_ERR_ARG;
+        if (t->leaf_kernel < 1 || t->leaf_kernel > 5) return PB_ERR_ARG;
         ctx->tuning.leaf_kernel = t->leaf_kernel;
     }
     if (t->leaf_blocks_per_sm) {
@@ -1615,6 +1696,10 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
             ctx->dtt.release();  // resized (and re-laid-out) on the next TT call
             ctx->dtt_max_depth = 0;
         }
+    }
+    if (t->planned_leaf) {
+        if (t->planned_leaf != 1 && t->planned_leaf != 2) return PB_ERR_ARG;
+        ctx->tuning.planned_leaf = t->planned_leaf;
     }
     return PB_OK;
 }

@@ -502,6 +502,71 @@ __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_sorted(const Board *__res
     }
 }
 
+// Ranked two-ply leaf whose grandchild counts iterate the child's own-piece
+// lists (ListedPieces) instead of scanning piece bitboards: every grandchild
+// of a child has the pieces of side C that the child has, less at most one
+// captured piece, so the knight and slider squares are listed once per child.
+// A child with more than four pieces of one kind counts with the bitboard
+// scans.  Same counts as k_leaf2_sorted.
+template <int C, bool STRICT, int T>
+__global__ void __launch_bounds__(T, 1024 / T) k_leaf2_listed(const Board *__restrict__ pboards,
+                                                              const uint8_t *__restrict__ pstates,
+                                                              const u32 *__restrict__ pidx,
+                                                              const uint16_t *__restrict__ moves, u64 n, u64 nparents,
+                                                              unsigned long long *__restrict__ counter)
+{
+    __shared__ Board s_b[T];
+    __shared__ uint8_t s_st[T];
+    __shared__ uint8_t s_key[T];  // 0 = no child, else 1 + its move count
+    const int tid = threadIdx.x;
+    const u64 i = (u64)blockIdx.x * T + tid;
+    Board b{};
+    u32 st = 0, key = 0;
+    if (i < n && pidx[i] < nparents) {
+        u32 p = pidx[i];
+        b = load_board(pboards + p);
+        st = pstates[p];
+        make_move<C>(b, st, moves[i]);
+        key = 1 + min(count_moves<1 - C, true>(b, st), 254u);
+    }
+    const u32 rank = cta_rank_u8<T>(key);
+    s_b[rank] = b;
+    s_st[rank] = (uint8_t)st;
+    s_key[rank] = (uint8_t)key;
+    __syncthreads();
+    u32 total = 0, counted = 0;
+    if (s_key[tid]) {
+        b = s_b[tid];
+        st = s_st[tid];
+        uint16_t mv[MAX_MOVES];
+        ArraySink sink{mv, 0};
+        gen_moves<1 - C>(b, st, sink);
+        ListedPieces own;
+        if (own.build<C>(b)) {
+            for (int k = 0; k < sink.n; k++) {
+                Board g = b;
+                u32 gs = st;
+                make_move<1 - C>(g, gs, mv[k]);
+                total += count_moves<C, STRICT>(g, gs, own);
+            }
+        } else {
+            for (int k = 0; k < sink.n; k++) {
+                Board g = b;
+                u32 gs = st;
+                make_move<1 - C>(g, gs, mv[k]);
+                total += count_moves<C, STRICT>(g, gs);
+            }
+        }
+        counted = sink.n;
+    }
+    total = __reduce_add_sync(0xffffffffu, total);
+    counted = __reduce_add_sync(0xffffffffu, counted);
+    if ((tid & 31) == 0 && counted) {
+        atomicAdd(counter, (unsigned long long)total);
+        atomicAdd(counter + 1, (unsigned long long)counted);
+    }
+}
+
 // ---------------------------------------------------------------- cooperative leaf
 // Fused two-ply leaf with the grandchild work spread over the whole CTA.
 //
@@ -719,12 +784,12 @@ __device__ __forceinline__ void rank_children(Board &b, u32 &st, u32 &root, bool
 // Two-ply leaf over edges, counts credited to each edge's root.  With SORT
 // the CTA's children are ranked by move count first (blockDim.x must be
 // PB_LEAF_THREADS).
-template <int C, bool STRICT, bool SORT = false>
-__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
-    k_leaf2_rooted(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
-                   const u32 *__restrict__ proot, const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
-                   u64 n, u64 nparents, unsigned long long *__restrict__ root_counts,
-                   unsigned long long *__restrict__ counter)
+template <int C, bool STRICT, bool SORT>
+__device__ __forceinline__ void leaf2_rooted_cta(const Board *__restrict__ pboards,
+                                                 const uint8_t *__restrict__ pstates, const u32 *__restrict__ proot,
+                                                 const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
+                                                 u64 n, u64 nparents, unsigned long long *__restrict__ root_counts,
+                                                 unsigned long long *__restrict__ counter)
 {
     u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     u32 total = 0, counted = 0, root = 0;
@@ -754,6 +819,16 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     add_by_key(root_counts, root, total, valid);
     counted = __reduce_add_sync(0xffffffffu, counted);
     if ((threadIdx.x & 31) == 0 && counted) atomicAdd(counter + 1, (unsigned long long)counted);
+}
+
+template <int C, bool STRICT, bool SORT = false>
+__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
+    k_leaf2_rooted(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                   const u32 *__restrict__ proot, const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
+                   u64 n, u64 nparents, unsigned long long *__restrict__ root_counts,
+                   unsigned long long *__restrict__ counter)
+{
+    leaf2_rooted_cta<C, STRICT, SORT>(pboards, pstates, proot, pidx, moves, n, nparents, root_counts, counter);
 }
 
 // One-ply leaf over edges (perft 1 of each edge's child), per root.
@@ -799,6 +874,24 @@ __device__ __forceinline__ u64 dev_size(const u64 *n_dev, u64 cap, u32 *err)
         n = cap;
     }
     return n;
+}
+
+// The same leaf with the level sizes in device memory, for captured graphs:
+// the grid covers the planned capacity and the CTAs past the level's actual
+// size leave at once (a whole CTA at a time, so the ranking's barriers are
+// reached by all of its threads or by none).
+template <int C, bool STRICT, bool SORT = false>
+__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
+    k_leaf2_rooted_dev(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                       const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
+                       const uint16_t *__restrict__ moves, const u64 *__restrict__ n_dev, u64 cap,
+                       const u64 *__restrict__ npar_dev, u64 npar_cap, unsigned long long *__restrict__ root_counts,
+                       unsigned long long *__restrict__ counter, u32 *__restrict__ err)
+{
+    const u64 n = dev_size(n_dev, cap, err);
+    if ((u64)blockIdx.x * blockDim.x >= n) return;
+    const u64 npar = min(*npar_dev, npar_cap);
+    leaf2_rooted_cta<C, STRICT, SORT>(pboards, pstates, proot, pidx, moves, n, npar, root_counts, counter);
 }
 
 // Scan with a device-resident length (grid = tiles of the capacity; surplus

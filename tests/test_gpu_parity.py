@@ -49,7 +49,7 @@ def test_scan_unaligned_and_many_tiles(gpu_engine):
         assert int(d_tot.item()) == int(x.sum()), (n, shift)
 
 
-@pytest.mark.parametrize("leaf_kernel", [1, 2, 4])
+@pytest.mark.parametrize("leaf_kernel", [1, 2, 4, 5])
 def test_gpu_matches_reference_fixtures(gpu_engine, golden, leaf_kernel):
     prev = gpu_engine.get_tuning().leaf_kernel
     gpu_engine.set_tuning(leaf_kernel=leaf_kernel)
@@ -89,7 +89,7 @@ def test_strict_mode_counts_merged_moves(oracle):
     comp.close()
 
 
-@pytest.mark.parametrize("leaf_kernel", [1, 2, 4])
+@pytest.mark.parametrize("leaf_kernel", [1, 2, 4, 5])
 def test_readme_known_totals(gpu_engine, leaf_kernel):
     # README.md:51-52 and :92 (RTX PRO 6000 / GB10 tables)
     prev = gpu_engine.get_tuning().leaf_kernel
@@ -258,4 +258,24 @@ def test_batched_leaf_ranked_and_unranked_agree():
     plain = eng.perft_batch(roots, depths)
     assert ranked == plain
     assert ranked == [eng.perft_position(r, d) for r, d in zip(roots, depths)]
+    eng.close()
+
+
+@pytest.mark.parametrize("threads", [128, 256, 512])
+def test_listed_piece_leaf_on_playouts(threads, oracle):
+    """Leaf kernel 5 (own-piece squares listed once per child) against the
+    oracle on playout positions of every game phase, both colours to move,
+    including positions with promoted pieces (more than four of a kind fall
+    back to the bitboard count)."""
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
+    eng.set_tuning(leaf_kernel=5, leaf_threads=threads)
+    roots = [p for p in pg.random_playouts(4747, 40, 0, 160) if pg.count_moves(p, True) > 0]
+    for p in roots:
+        fen = pg.to_fen(p)
+        assert eng.perft_position(p, 4) == oracle.perft(fen, 4), fen
+    # five queens and five knights: the listed side has more than four of a
+    # kind at odd depths (white's pieces are listed) and none at even depths
+    many = "7k/8/8/8/8/8/NNNNN3/QQQQQ1K1 w - - 0 1"
+    for d in (3, 4, 5):
+        assert eng.perft_position(pg.parse_fen(many), d) == oracle.perft(many, d), d
     eng.close()

@@ -254,3 +254,19 @@ def test_u128_accumulation_and_text_across_2_64():
     for v in parts:
         acc = pg.u128_add(acc, v)
     assert pg.u128_text(acc) == "61885021521585529237"
+
+
+def test_listed_piece_counts_equal_bitboard_counts(golden):
+    """The listed-piece counter of leaf kernel 5 (the side's knight and slider
+    squares listed once per parent position) against the bitboard counter on
+    every child of playout positions and of the fixture positions (pins,
+    captures of listed pieces, checks, promotions, castling, en passant)."""
+    positions = [pg.parse_fen(c["fen"]) for c in golden]
+    positions += pg.random_playouts(31337, 6000, 0, 120)
+    # grandchildren of the fixtures as parents too: more pinned and captured pieces
+    for c in golden[:20]:
+        p = pg.parse_fen(c["fen"])
+        positions += [pg.make_move(p, m) for m in pg.generate_moves(p)]
+    checked, bad = pg.selftest_listed_counts(positions)
+    assert bad == 0
+    assert checked > 100_000
