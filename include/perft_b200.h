@@ -195,7 +195,10 @@ typedef struct {
     int planned_leaf;   /* leaf of planned (graph-captured) batches: 1 = grid over the planned
                            capacity, CTAs past the level's size leave at once (default);
                            2 = persistent CTAs fed by an atomic work queue */
-    int reserved;
+    int host_driver;    /* tree above the launch depth in pb_perft_launch: 1 = depth first, one GPU
+                           call per subtree (perft_cpu_recurse, launcher.cu:572-715; default);
+                           2 = breadth first, transpositions merged by key with tables, the
+                           launch-depth positions in batched GPU calls */
 } pb_tuning;
 
 int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t);

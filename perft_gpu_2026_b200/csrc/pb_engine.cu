@@ -19,6 +19,7 @@
 #include <chrono>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -72,7 +73,7 @@ struct pb_ctx {
     u64 *h_pinned = nullptr;  // pinned host words for readbacks
     int launch_depth = 0;
     bool timing = false;
-    pb_tuning tuning{4, 0, 256, 128, 2, 1, 1, 0};
+    pb_tuning tuning{4, 0, 256, 128, 2, 1, 1, 1};
     int num_sms = 0;
     uint16_t *spill = nullptr;  // cooperative-leaf spill area (device)
     size_t spill_blocks = 0;
@@ -86,6 +87,7 @@ struct pb_ctx {
     size_t dtt_free_bytes = 0;
     u32 dedup_gen = 0;
     int htt_last = 0;
+    u64 tt_batch = 1;  // roots per batched table-mode call that fit last time
     std::string err;
 };
 
@@ -423,56 +425,116 @@ struct TTLevel {
     int rem;
 };
 
-// One GPU breadth-first perft with the device TTs (perft_gpu_host_bfs with
-// g_useTT, perft_kernels.cu:620-990): probe at every level, dedup, leaf TT,
-// then the upsweep stores every level's counts.
-int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth, const Hash128 &root_hash,
-                 u64 *out, int *bfs_status)
+// GPU breadth-first perft with the device TTs (perft_gpu_host_bfs with
+// g_useTT, perft_kernels.cu:620-990) of n roots of one colour at once: probe
+// at every level, dedup (across all the roots' subtrees of a level), leaf TT,
+// then the upsweep stores every level's counts and a last upsweep over the
+// roots' own moves gives each root's count.  out[k] = perft(depth) of root k.
+int bfs_tt_roots(pb_ctx *ctx, const Board *rb, const uint8_t *rs, const Hash128 *rh, u64 nroots, int color,
+                 int depth, u64 *out, int *bfs_status)
 {
     NvtxRange nvtx_pass("bfs_perft_tt");
     *bfs_status = BFS_OK;
     const bool strict = ctx->opts.strict != 0;
+    if (nroots == 0) return PB_OK;
     if (depth <= 2) {
-        *out = host_perft(root, root_st, color, depth, strict);
+        for (u64 k = 0; k < nroots; k++) out[k] = host_perft(rb[k], rs[k], color, depth, strict);
         return PB_OK;
     }
     int rc = ensure_dtt(ctx, depth - 1);
     if (rc != PB_OK) return rc;
-    uint16_t root_moves[MAX_MOVES];
-    int n0 = host_gen(root, root_st, color, root_moves);
-    if (n0 == 0) {
-        *out = 0;
-        return PB_OK;
-    }
     cudaStream_t s = ctx->stream;
     pb_stats &stats = ctx->stats;
     Arena ar{ctx->arena, ctx->arena_bytes};
-    Board *pb_ = ar.take<Board>(1);
-    uint8_t *ps = ar.take<uint8_t>(1);
-    Hash128 *ph = ar.take<Hash128>(1);
-    uint16_t *emv = ar.take<uint16_t>(n0);
-    u32 *epi = ar.take<u32>(n0);
-    if (!pb_ || !ps || !ph || !emv || !epi) {
+    Board *pb_ = ar.take<Board>(nroots);
+    uint8_t *ps = ar.take<uint8_t>(nroots);
+    Hash128 *ph = ar.take<Hash128>(nroots);
+    u32 *rcnt = ar.take<u32>(nroots);       // root move counts
+    u64 *roff = ar.take<u64>(nroots);       // root edge offsets
+    uint8_t *rflags = ar.take<uint8_t>(nroots);
+    u64 *rvals = ar.take<u64>(nroots);
+    if (!pb_ || !ps || !ph || !rcnt || !roff || !rflags || !rvals) {
         *bfs_status = BFS_TOO_BIG;
         return PB_OK;
     }
-    uint8_t st8 = (uint8_t)root_st;
-    PB_CUDA(cudaMemcpyAsync(pb_, &root, sizeof(Board), cudaMemcpyHostToDevice, s));
-    PB_CUDA(cudaMemcpyAsync(ps, &st8, 1, cudaMemcpyHostToDevice, s));
-    PB_CUDA(cudaMemcpyAsync(ph, &root_hash, sizeof(Hash128), cudaMemcpyHostToDevice, s));
-    PB_CUDA(cudaMemcpyAsync(emv, root_moves, sizeof(uint16_t) * n0, cudaMemcpyHostToDevice, s));
-    PB_CUDA(cudaMemsetAsync(epi, 0, sizeof(u32) * n0, s));
+    std::vector<uint8_t> st8(rs, rs + nroots);
+    PB_CUDA(cudaMemcpyAsync(pb_, rb, sizeof(Board) * nroots, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(ps, st8.data(), nroots, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(ph, rh, sizeof(Hash128) * nroots, cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemsetAsync(rflags, 0, nroots, s));
     PB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(u32), s));
-    stats.h2d_bytes += sizeof(Board) + 1 + sizeof(Hash128) + sizeof(uint16_t) * n0;
+    stats.h2d_bytes += (sizeof(Board) + 1 + sizeof(Hash128)) * nroots;
     if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[0], s));
+
+    // the roots' moves: from the host for one root, else counted, scanned and
+    // generated on the device like every other level
+    uint16_t *emv = nullptr;
+    u32 *epi = nullptr;
+    u64 n = 0;
+    if (nroots == 1) {
+        uint16_t root_moves[MAX_MOVES];
+        int n0 = host_gen(rb[0], rs[0], color, root_moves);
+        n = (u64)n0;
+        emv = ar.take<uint16_t>(n ? n : 1);
+        epi = ar.take<u32>(n ? n : 1);
+        if (!emv || !epi) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        u32 c0 = (u32)n0;
+        u64 z = 0;
+        PB_CUDA(cudaMemcpyAsync(rcnt, &c0, sizeof(u32), cudaMemcpyHostToDevice, s));
+        PB_CUDA(cudaMemcpyAsync(roff, &z, sizeof(u64), cudaMemcpyHostToDevice, s));
+        if (n) {
+            PB_CUDA(cudaMemcpyAsync(emv, root_moves, sizeof(uint16_t) * n, cudaMemcpyHostToDevice, s));
+            PB_CUDA(cudaMemsetAsync(epi, 0, sizeof(u32) * n, s));
+        }
+        stats.h2d_bytes += sizeof(uint16_t) * n + 12;
+    } else {
+        u64 tiles0 = (nroots + SCAN_TILE - 1) / SCAN_TILE;
+        u64 *status0 = ar.take<u64>(tiles0);
+        if (!status0) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        if (color == WHITE)
+            k_count_positions<WHITE, true><<<grid_for(nroots, 256), 256, 0, s>>>(pb_, ps, nroots, rcnt);
+        else
+            k_count_positions<BLACK, true><<<grid_for(nroots, 256), 256, 0, s>>>(pb_, ps, nroots, rcnt);
+        PB_CUDA(cudaMemsetAsync(status0, 0, sizeof(u64) * tiles0, s));
+        PB_CUDA(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), s));
+        k_scan<<<(unsigned)tiles0, SCAN_THREADS, 0, s>>>(rcnt, nroots, roff, status0, ctx->d_ticket, ctx->d_total,
+                                                          ctx->d_err);
+        PB_CUDA(cudaGetLastError());
+        PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_total, sizeof(u64), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+        stats.kernels += 2;
+        stats.d2h_bytes += 8;
+        n = ctx->h_pinned[0];
+        if (n > 0xFFFFFFFFULL) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        emv = ar.take<uint16_t>(n ? n : 1);
+        epi = ar.take<u32>(n ? n : 1);
+        if (!emv || !epi) {
+            *bfs_status = BFS_TOO_BIG;
+            return PB_OK;
+        }
+        if (n) {
+            launch_generate(ctx, color, pb_, ps, roff, nroots, emv, epi);
+            PB_CUDA(cudaGetLastError());
+            stats.kernels += 1;
+        }
+    }
 
     std::vector<TTLevel> levels;
     Board *cur_b = pb_;
     uint8_t *cur_s = ps;
     Hash128 *cur_h = ph;
-    u64 n = (u64)n0, n_par = 1;
+    u64 n_par = nroots;
     int c = color;
-    for (int rem = depth - 1; rem > 2; rem--) {
+    for (int rem = depth - 1; rem > 2 && n; rem--) {
         TTLevel L{};
         Board *cb = ar.take<Board>(n);
         uint8_t *cs = ar.take<uint8_t>(n);
@@ -590,7 +652,8 @@ int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int dep
         stats.kernels += 1;
     }
     if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[2], s));
-    // upsweep
+    // upsweep, deepest level first, then the roots (their counts are not
+    // stored: the root depth has no device table, the host keeps them)
     const u32 *child32 = leafcnt;
     const u64 *child64 = nullptr;
     for (int li = (int)levels.size() - 1; li >= 0; li--) {
@@ -606,22 +669,24 @@ int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int dep
         stats.kernels += 2;
         child64 = L.vals;
     }
-    PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
-    if (levels.empty())
-        k_sum<u32><<<grid_for(n, 256), 256, 0, s>>>(leafcnt, n, ctx->d_counter);
+    const TTView none{nullptr, 0, TT_NONE, 0};
+    if (child64)
+        k_upsweep<u64><<<grid_for(nroots, 256), 256, 0, s>>>(child64, roff, rcnt, rflags, ph, nroots, none, rvals);
     else
-        k_sum<u64><<<grid_for(levels[0].n, 256), 256, 0, s>>>(levels[0].vals, levels[0].n, ctx->d_counter);
+        k_upsweep<u32><<<grid_for(nroots, 256), 256, 0, s>>>(child32, roff, rcnt, rflags, ph, nroots, none, rvals);
     PB_CUDA(cudaGetLastError());
     stats.kernels += 1;
     if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[3], s));
+    std::vector<u64> tmp(nroots);
+    PB_CUDA(cudaMemcpyAsync(tmp.data(), rvals, sizeof(u64) * nroots, cudaMemcpyDeviceToHost, s));
     PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->d_counter, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s));
     PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 2, ctx->d_err, sizeof(u32), cudaMemcpyDeviceToHost, s));
     PB_CUDA(cudaStreamSynchronize(s));
     if ((u32)ctx->h_pinned[2]) return fail(ctx, PB_ERR_DEVICE, "TT kernel reported a device error");
-    *out = ctx->h_pinned[0];
+    for (u64 k = 0; k < nroots; k++) out[k] = tmp[k];
     stats.leaf_edges += n;
     stats.leaf_positions += ctx->h_pinned[1];
-    stats.d2h_bytes += 20;
+    stats.d2h_bytes += 8 * nroots + 20;
     if (ctx->timing) {
         float a = 0, b2 = 0;
         PB_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[3]));
@@ -630,6 +695,13 @@ int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int dep
         stats.leaf_ms += b2;
     }
     return PB_OK;
+}
+
+int bfs_perft_tt(pb_ctx *ctx, const Board &root, u32 root_st, int color, int depth, const Hash128 &root_hash,
+                 u64 *out, int *bfs_status)
+{
+    const uint8_t st8 = (uint8_t)root_st;
+    return bfs_tt_roots(ctx, &root, &st8, &root_hash, 1, color, depth, out, bfs_status);
 }
 
 // perft of one position on the GPU; a level too big for the arena splits the
@@ -1378,6 +1450,159 @@ int launch_recurse(pb_ctx *ctx, const Board &b, u32 st, int c, int depth, const 
     return PB_OK;
 }
 
+// Table-mode perft of n roots of one colour in batched GPU calls that fit the
+// arena: a batch whose levels do not fit is halved (a single root that does
+// not fit goes to the single-root path, which splits it on the host); the
+// batch size that fit last seeds the next call and doubles after a success.
+int gpu_tt_roots(pb_ctx *ctx, const Board *rb, const uint8_t *rs, const Hash128 *rh, u64 n, int color, int depth,
+                 u64 *out)
+{
+    u64 b = std::max<u64>(ctx->tt_batch, 1);
+    u64 i = 0;
+    while (i < n) {
+        const u64 m = std::min(b, n - i);
+        int status = BFS_OK;
+        int rc = bfs_tt_roots(ctx, rb + i, rs + i, rh + i, m, color, depth, out + i, &status);
+        if (rc != PB_OK) return rc;
+        if (status == BFS_OK) {
+            i += m;
+            if (m == b && b < (1u << 20)) b *= 2;
+            continue;
+        }
+        if (m == 1) {
+            rc = gpu_perft(ctx, rb[i], rs[i], color, depth, out + i);
+            if (rc != PB_OK) return rc;
+            i++;
+            continue;
+        }
+        b = m / 2;
+    }
+    ctx->tt_batch = b;
+    return PB_OK;
+}
+
+// Host driver above the launch depth, breadth first (pb_tuning.host_driver =
+// 2).  The reference walks the tree above the launch depth depth first and
+// makes one GPU call per subtree (perft_cpu_recurse, launcher.cu:572-715).
+// Here the tree is expanded on the host ply by ply down to the launch depth;
+// with tables, positions reached by several move orders are merged by their
+// 128-bit key (each keeps the number of paths that reach it) and positions
+// found in the host table are answered from it.  The positions left at the
+// launch depth then run in batched GPU calls, table mode with duplicates also
+// merged across the batch's subtrees at every level, and
+// perft = sum over them of paths x perft(launch depth), in 128 bits.  Without
+// tables nothing is merged (no key is computed) and the batches run through
+// the count-then-allocate batched path.
+struct HostNode {
+    Board b;
+    uint8_t s;
+    Hash128 h;
+    u64 paths;
+};
+struct KeyHash {
+    size_t operator()(const Hash128 &h) const { return (size_t)(h.lo ^ (h.hi * 0x9E3779B97F4A7C15ULL)); }
+};
+struct KeyEq {
+    bool operator()(const Hash128 &a, const Hash128 &b) const { return a.lo == b.lo && a.hi == b.hi; }
+};
+
+inline void add_product(pb_u128 &acc, u64 a, u64 b)
+{
+    unsigned __int128 p = (unsigned __int128)a * b;
+    pb_u128 v{(u64)p, (u64)(p >> 64)};
+    add128(acc, v);
+}
+
+int launch_breadth_first(pb_ctx *ctx, const Board &root, u32 root_st, int c, int depth, const Hash128 &root_h,
+                         pb_u128 *out)
+{
+    const bool tt = ctx->opts.use_tt && ctx->htt.ready();
+    const int ld = ctx->launch_depth;
+    pb_u128 total{0, 0};
+    std::vector<HostNode> level{HostNode{root, (uint8_t)root_st, root_h, 1}};
+    int col = c;
+    constexpr size_t MAX_HOST_NODES = 1u << 22;
+    for (int rem = depth; rem > ld && !level.empty(); rem--) {
+        std::vector<HostNode> next;
+        std::unordered_map<Hash128, u32, KeyHash, KeyEq> index;
+        for (const HostNode &nd : level) {
+            uint16_t mv[MAX_MOVES];
+            int m = host_gen(nd.b, nd.s, col, mv);
+            for (int k = 0; k < m; k++) {
+                HostNode ch{nd.b, nd.s, Hash128{0, 0}, nd.paths};
+                u32 cs = nd.s;
+                host_make(ch.b, cs, col, mv[k]);
+                ch.s = (uint8_t)cs;
+                if (tt) {
+                    ch.h = hash_move(nd.h, nd.b, nd.s, cs, col, mv[k]);
+                    auto it = index.find(ch.h);
+                    if (it != index.end()) {
+                        next[it->second].paths += nd.paths;
+                        continue;
+                    }
+                    index.emplace(ch.h, (u32)next.size());
+                }
+                next.push_back(ch);
+            }
+            if (next.size() > MAX_HOST_NODES) {
+                // too wide to hold: walk this call depth first instead
+                return launch_recurse(ctx, root, root_st, c, depth, root_h, out);
+            }
+        }
+        col = 1 - col;
+        if (tt) {
+            // answered by the host table at this remaining depth
+            std::vector<HostNode> keep;
+            keep.reserve(next.size());
+            for (const HostNode &nd : next) {
+                u64 hit;
+                if (rem - 1 >= 2 && ctx->htt.probe(rem - 1, nd.h, &hit))
+                    add_product(total, nd.paths, hit);
+                else
+                    keep.push_back(nd);
+            }
+            next.swap(keep);
+        }
+        level.swap(next);
+    }
+    const int d = std::min(ld, depth);
+    const u64 n = level.size();
+    if (n) {
+        std::vector<u64> vals(n, 0);
+        int rc = PB_OK;
+        if (!ctx->gpu) {
+            for (u64 k = 0; k < n; k++) vals[k] = host_perft(level[k].b, level[k].s, col, d, ctx->opts.strict != 0);
+        } else if (ctx->opts.use_tt) {
+            std::vector<Board> rb(n);
+            std::vector<uint8_t> rs(n);
+            std::vector<Hash128> rh(n);
+            for (u64 k = 0; k < n; k++) {
+                rb[k] = level[k].b;
+                rs[k] = level[k].s;
+                rh[k] = level[k].h;
+            }
+            rc = gpu_tt_roots(ctx, rb.data(), rs.data(), rh.data(), n, col, d, vals.data());
+        } else {
+            // count-then-allocate batches of white-to-move roots
+            std::vector<Board> rb(n);
+            std::vector<uint8_t> rs(n);
+            for (u64 k = 0; k < n; k++) {
+                pb_pos p;
+                to_pos(level[k].b, level[k].s, col, p);
+                to_white_to_move(p, rb[k], rs[k]);
+            }
+            rc = gpu_batch(ctx, rb.data(), rs.data(), n, d, vals.data());
+        }
+        if (rc != PB_OK) return rc;
+        for (u64 k = 0; k < n; k++) {
+            add_product(total, level[k].paths, vals[k]);
+            if (tt && d >= 2) ctx->htt.store(d, level[k].h, vals[k]);
+        }
+    }
+    *out = total;
+    return PB_OK;
+}
+
 // Listed-piece counting against the bitboard counter on every child of
 // `y` (side Z to move): the lists of side 1-Z are taken from y, as the fused
 // leaf takes them from its child position.  Compares both counters (reference
@@ -1701,6 +1926,10 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
         if (t->planned_leaf != 1 && t->planned_leaf != 2) return PB_ERR_ARG;
         ctx->tuning.planned_leaf = t->planned_leaf;
     }
+    if (t->host_driver) {
+        if (t->host_driver != 1 && t->host_driver != 2) return PB_ERR_ARG;
+        ctx->tuning.host_driver = t->host_driver;
+    }
     return PB_OK;
 }
 
@@ -1774,7 +2003,19 @@ int pb_perft_launch(pb_ctx *ctx, const pb_pos *pos, int depth, pb_u128 *count, d
         rc = PB_OK;
     } else {
         Hash128 h = ctx->opts.use_tt ? hash_position(b, pos->state, pos->color) : Hash128{0, 0};
-        rc = launch_recurse(ctx, b, pos->state, pos->color, depth, h, &r);
+        const bool tt = ctx->opts.use_tt && ctx->htt.ready();
+        u64 hit = 0;
+        if (ctx->tuning.host_driver == 2 && depth > ctx->launch_depth) {
+            if (tt && ctx->htt.probe(depth, h, &hit)) {
+                r.lo = hit;
+                rc = PB_OK;
+            } else {
+                rc = launch_breadth_first(ctx, b, pos->state, pos->color, depth, h, &r);
+                if (rc == PB_OK && tt && r.hi == 0) ctx->htt.store(depth, h, r.lo);
+            }
+        } else {
+            rc = launch_recurse(ctx, b, pos->state, pos->color, depth, h, &r);
+        }
     }
     auto t1 = std::chrono::steady_clock::now();
     if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();

@@ -228,9 +228,23 @@ static int journaled_depth(pb_ctx *ctx, const pb_pos &root, const std::string &f
     return PB_OK;
 }
 
+// -hd: host driver above the launch depth (1 = depth first, 2 = breadth
+// first with batched GPU calls); -lk: leaf kernel.  0 keeps the default.
+static int apply_tuning(pb_ctx *ctx, int host_driver, int leaf_kernel)
+{
+    pb_tuning t;
+    memset(&t, 0, sizeof(t));
+    t.host_driver = host_driver;
+    t.leaf_kernel = leaf_kernel;
+    int rc = pb_set_tuning(ctx, &t);
+    if (rc != PB_OK) fprintf(stderr, "invalid -hd or -lk value\n");
+    return rc;
+}
+
 int main(int argc, char **argv)
 {
     bool cpu = false, json = false;
+    int host_driver = 0, leaf_kernel = 0;
     std::string batch_file, journal;
     pb_opts opts;
     pb_default_opts(&opts);
@@ -246,6 +260,8 @@ int main(int argc, char **argv)
         else if (a == "-ld" && i + 1 < argc) opts.launch_depth = atoi(argv[++i]);
         else if (a == "-dtt" && i + 1 < argc) opts.device_tt_mb = atoi(argv[++i]);
         else if (a == "-htt" && i + 1 < argc) opts.host_tt_mb = atoi(argv[++i]);
+        else if (a == "-hd" && i + 1 < argc) host_driver = atoi(argv[++i]);
+        else if (a == "-lk" && i + 1 < argc) leaf_kernel = atoi(argv[++i]);
         else pos.push_back(a);
     }
     if (!batch_file.empty()) return run_batch(batch_file, pos.empty() ? 0 : atoi(pos[0].c_str()), cpu, json, opts);
@@ -257,7 +273,7 @@ int main(int argc, char **argv)
         if (pos.size() >= 3 && opts.launch_depth == 0) opts.launch_depth = atoi(pos[2].c_str());
     } else {
         printf("\nUsage: perft_gpu <fen> <depth> [<launchdepth>] [-nott] [-dtt <MB>] [-htt <MB>] [-ld <N>] [-cpu] [-strict]"
-               " [-json] [-journal <file>]\n");
+               " [-json] [-journal <file>] [-hd 1|2] [-lk <leaf kernel>]\n");
         printf("\nAs no parameters were provided... running default test\n");
     }
     pb_pos root;
@@ -275,6 +291,7 @@ int main(int argc, char **argv)
         fflush(stdout);
         opts.use_tt = 0;
         if (pb_create(-1, &opts, &ctx) != PB_OK) return 1;
+        if (apply_tuning(ctx, host_driver, leaf_kernel) != PB_OK) return 1;
         for (int d = 1; d <= max_depth; d++) {
             pb_u128 v;
             double secs = 0;
@@ -305,6 +322,7 @@ int main(int argc, char **argv)
         fprintf(stderr, "init failed (%d)\n", rc);
         return 1;
     }
+    if (apply_tuning(ctx, host_driver, leaf_kernel) != PB_OK) return 1;
     printf("Launch depth: %d\n", pb_prepare(ctx, &root, max_depth));
     fflush(stdout);
     for (int d = 1; d <= max_depth; d++) {

@@ -131,6 +131,8 @@ def test_config5_tables_equal_no_tables_and_reference(fixture):
     tt = _lines(CLI, [c["fen"], "9", "-dtt", "150000", "-htt", "16384"])
     nott = _lines(CLI, [c["fen"], "9", "-nott"])
     assert tt == nott
+    # the breadth-first host driver with batched table-mode GPU calls
+    assert _lines(CLI, [c["fen"], "9", "-dtt", "150000", "-htt", "16384", "-hd", "2", "-ld", "6"]) == tt
     assert tt[:len(c["counts"])] == c["counts"]
     if os.path.exists(REF):
         assert _lines(REF, [c["fen"], "9", "-dtt", "150000", "-htt", "16384"]) == tt

@@ -85,3 +85,30 @@ def test_size_priority_buckets_stay_exact():
     assert small.perft_position(pg.parse_fen(KIWIPETE), 5) == 193690690
     small.close()
     eng.close()
+
+
+@pytest.mark.parametrize("use_tt", [True, False])
+def test_breadth_first_host_driver_on_the_gpu(use_tt):
+    """host_driver 2: the tree above the launch depth expanded ply by ply,
+    transpositions merged by key with tables, the launch-depth positions in
+    batched GPU calls (table mode: duplicates merged across the batch's
+    subtrees too).  Equal to the depth-first driver and the known totals,
+    also with an arena so small that batches must be halved."""
+    for arena, ld in ((2 << 30, 5), (96 << 20, 4)):
+        eng = pg.Engine(device=0, use_tt=use_tt, arena_bytes=arena, device_tt_mb=1024, host_tt_mb=256,
+                        launch_depth=ld)
+        eng.set_tuning(host_driver=2)
+        res = eng.perft(START, 8)
+        assert [r for r, _ in res] == [20, 400, 8902, 197281, 4865609, 119060324, 3195901860, 84998978956]
+        got, _ = eng.perft_launch(pg.parse_fen(KIWIPETE), 6)
+        assert got == 8031647685
+        eng.close()
+    eng = pg.Engine(device=0, use_tt=use_tt, arena_bytes=2 << 30, device_tt_mb=1024, host_tt_mb=256, launch_depth=4)
+    eng.set_tuning(host_driver=2)
+    ref = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
+    for seed in range(4):
+        p = pg.config_position(10 + 3 * seed, 500 + seed)
+        got, _ = eng.perft_launch(p, 7)
+        assert got == ref.perft_position(p, 7)
+    ref.close()
+    eng.close()

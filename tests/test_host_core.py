@@ -270,3 +270,25 @@ def test_listed_piece_counts_equal_bitboard_counts(golden):
     checked, bad = pg.selftest_listed_counts(positions)
     assert bad == 0
     assert checked > 100_000
+
+
+@pytest.mark.parametrize("use_tt", [False, True])
+def test_breadth_first_host_driver(use_tt, golden):
+    """host_driver 2: the tree above the launch depth expanded ply by ply
+    (transpositions merged by key, each with its path count, when tables are
+    on) must give the depth-first driver's counts (perft_cpu_recurse order)
+    on a host-only context, and the known totals."""
+    kiwi = "r3k2r/p1ppqpb1/bn2pnp1/3PN3/1p2P3/2N2Q1p/PPPBBPPP/R3K2R w KQkq -"
+    cases = [(pg.START_FEN, 5, 4_865_609), (kiwi, 4, 4_085_603)]
+    cases += [(c["fen"], len(c["counts"]), c["counts"][-1]) for c in golden[:12] if c["counts"][-1] < 3_000_000]
+    for ld in (1, 2, 3):
+        bf = pg.Engine(device=-1, use_tt=use_tt, launch_depth=ld, host_tt_mb=64)
+        bf.set_tuning(host_driver=2)
+        df = pg.Engine(device=-1, use_tt=use_tt, launch_depth=ld, host_tt_mb=64)
+        for fen, depth, want in cases:
+            p = pg.parse_fen(fen)
+            got, _ = bf.perft_launch(p, depth)
+            ref, _ = df.perft_launch(p, depth)
+            assert got == ref == want, (fen, depth, ld, got, ref)
+        bf.close()
+        df.close()
