@@ -22,8 +22,14 @@ Printed JSON line (rank 0):
   reference_gpu  the reference's own GPU build (oracle/_ref, sm_100a) on the
            same position and depth, one GPU call (launch depth 7), timed by
            the reference program itself
+  scheduler  (one GPU) the learned scheduler: trained on 2^20 positions,
+           held-out prediction error per depth, and planned vs
+           count-then-allocate vs plain seconds on held-out roots at depths 4..7
   positions  (one GPU) positions/s on 4096 uneven roots at perft 5: plain
            per-root calls, count-then-allocate batch, learned planner
+  tt_run   (one GPU) perft 10 of the 2-ply seed-4 position with 150 GB of
+           device tables: host drivers and replacement policies beside the
+           reference's own table build
 `config` is the same dict in both arms (--impl engine and reference).
 With --gpus N > 1 (torchrun, one process per GPU) the depth-2 subtrees of the
 root are bin-packed over the ranks by their perft(2) (strong scaling: total
@@ -244,50 +250,143 @@ def reference_gpu(fen, depth, reps=3):
                       "sm_100a), the time it prints for the depth line, best of the runs"}
 
 
+def _timed(fn, reps):
+    """Best host wall time of `reps` calls after one warm-up call."""
+    fn()
+    best, out = None, None
+    for _ in range(reps):
+        t = time.perf_counter()
+        out = fn()
+        dt = time.perf_counter() - t
+        best = dt if best is None else min(best, dt)
+    return out, best
+
+
+def scheduler_section(pg, eng, train_n=1 << 20, eval_n=16384, timed_n=1024):
+    """The learned scheduler (config 4).  Training set: `train_n` playouts of
+    0..60 plies (splitmix64 seed 3, positions with a legal move) labelled with
+    exact perft 1..4 by batched GPU passes; the network (781 -> 256 -> 256 ->
+    4, BF16 weights, FP32 accumulation, Adam) trained by the library's own
+    kernels for 12 epochs.  Held out: `eval_n` playouts (seed 3003) with
+    depths uniform in 4..7 (seed 3004): mean absolute error of the predicted
+    log2(1 + perft(k)) per k against the exact labels (and of a constant guess,
+    the training mean), then the first `timed_n` of them counted three ways
+    through the public API: one plain call per root, count-then-allocate
+    batches, and the planned batches (predicted level sizes, bin-packing, one
+    captured graph per batch).  All three must agree."""
+    import numpy as np
+    from perft_gpu_2026_b200 import scheduler
+
+    t0 = time.perf_counter()
+    pos, y, _ = scheduler.make_training_set(eng, train_n)
+    t_label = time.perf_counter() - t0
+    eng.mlp_init(seed=1, out_bias=list(y.mean(0)))
+    t1 = time.perf_counter()
+    loss = eng.mlp_train(pos, y, epochs=12, batch=4096, lr=2e-3)
+    t_train = time.perf_counter() - t1
+    held = scheduler.keep_movable(pg.random_playouts(3003, eval_n + eval_n // 8, 0, 60))[:eval_n]
+    depths = scheduler.eval_depths(len(held))
+    truth = np.log2(1.0 + scheduler.label(eng, held))
+    pred = eng.mlp_predict(held)
+    mae = np.abs(pred - truth).mean(0).tolist()
+    mae_const = np.abs(y.mean(0)[None, :] - truth).mean(0).tolist()
+    sub, dsub = held[:timed_n], depths[:timed_n]
+    t = time.perf_counter()
+    plain = [eng.perft_position(p, d) for p, d in zip(sub, dsub)]
+    t_plain = time.perf_counter() - t
+    t = time.perf_counter()
+    batched = eng.perft_batch(sub, dsub)
+    t_batched = time.perf_counter() - t
+    t = time.perf_counter()
+    planned, st = eng.perft_batch_planned(sub, dsub)
+    t_planned = time.perf_counter() - t
+    assert plain == batched == list(planned), "scheduler evaluation: counts differ between modes"
+    return {"workload": f"{len(pos)} training positions (0..60-ply playouts, seed 3), {len(held)} held-out "
+                        f"(seed 3003) at depths U[4,7] (seed 3004), the first {len(sub)} timed",
+            "label_s": t_label, "train_s": t_train, "train_mse": loss,
+            "mae_log2_perft1_4": mae, "mae_log2_perft1_4_constant_guess": mae_const,
+            "timed": {"roots": len(sub), "nodes": int(sum(plain)), "plain_s": t_plain, "batched_s": t_batched,
+                      "learned_s": t_planned, "learned_vs_batched": t_batched / t_planned,
+                      "learned_vs_plain": t_plain / t_planned,
+                      "plan": {"batches": st.batches, "graph_batches": st.graph_batches, "retries": st.retries,
+                               "split_roots": st.split_roots},
+                      "timing": "host wall clock around the public call, one run each"}}
+
+
 def positions_section(pg, eng, reps):
     """Positions/s on 4096 uneven roots (playouts of 6..40 plies, splitmix64
     seed 2), perft 5 each, three ways through the public API (roots in host
     memory, counts read back, host wall clock): one plain call per root, one
-    count-then-allocate batched call, and the learned planner (network trained
-    here by the library's own kernels on 2^18 playout positions of 0..60 plies,
-    seed 3, labelled with exact perft 1..4).  All three must agree."""
+    count-then-allocate batched call, and the learned planner (the network
+    scheduler_section trained).  Also the planner at perft 3 and 4 of the same
+    roots, where each batch's per-level host round trips are a larger share.
+    All modes must agree."""
     import numpy as np
     from perft_gpu_2026_b200 import scheduler
 
     roots = pg.uneven_roots(4096, 6, 40, seed=2)
     depths = [5] * len(roots)
-    t0 = time.perf_counter()
-    pos, y, _ = scheduler.make_training_set(eng, 1 << 18)
-    eng.mlp_init(seed=1, out_bias=list(y.mean(0)))
-    loss = eng.mlp_train(pos, y, epochs=12, batch=4096, lr=2e-3)
-    train_s = time.perf_counter() - t0
     truth = np.log2(1.0 + scheduler.label(eng, roots))
     mae = np.abs(eng.mlp_predict(roots) - truth).mean(0).tolist()
-
-    def timed(fn):
-        fn()  # warm-up (graph capture, arena growth)
-        best, out = None, None
-        for _ in range(reps):
-            t = time.perf_counter()
-            out = fn()
-            dt = time.perf_counter() - t
-            best = dt if best is None else min(best, dt)
-        return out, best
-
-    plain, t_plain = timed(lambda: [eng.perft_position(r, 5) for r in roots])
-    batched, t_batched = timed(lambda: eng.perft_batch(roots, depths))
-    (learned, plan), t_learned = timed(lambda: eng.perft_batch_planned(roots, depths))
+    plain, t_plain = _timed(lambda: [eng.perft_position(r, 5) for r in roots], reps)
+    batched, t_batched = _timed(lambda: eng.perft_batch(roots, depths), reps)
+    (learned, plan), t_learned = _timed(lambda: eng.perft_batch_planned(roots, depths), reps)
     assert plain == batched == list(learned), "batched or planned counts differ from the plain path"
     n = len(roots)
+    shallow = {}
+    for d in (3, 4):
+        b, tb = _timed(lambda: eng.perft_batch(roots, [d] * n), 5)
+        (l, _), tl = _timed(lambda: eng.perft_batch_planned(roots, [d] * n), 5)
+        assert b == list(l)
+        shallow[f"perft{d}"] = {"batched": n / tb, "learned": n / tl, "learned_vs_batched": tb / tl}
     return {"workload": "4096 uneven roots (6..40-ply playouts, seed 2), perft 5 each, no TT",
             "unit": "positions/s", "timing": "host wall clock around the public call, best of "
                                              f"{reps} after one warm-up",
             "nodes": int(sum(plain)), "plain": n / t_plain, "batched": n / t_batched, "learned": n / t_learned,
             "learned_vs_plain": t_plain / t_learned, "batched_vs_plain": t_plain / t_batched,
+            "learned_vs_batched": t_batched / t_learned,
             "plan": {"batches": plan.batches, "graph_batches": plan.graph_batches, "retries": plan.retries,
                      "split_roots": plan.split_roots},
-            "scheduler": {"train_positions": len(pos), "train_mse": loss, "train_s": train_s,
-                          "mae_log2_perft1_4_on_roots": mae}}
+            "mae_log2_perft1_4_on_roots": mae, "shallow_depths": shallow}
+
+
+def tt_section(pg, depth=10, dtt_mb=150000, htt_mb=16384, bf_launch_depth=8):
+    """The deep table run (config 5): the position 2 random plies from the
+    initial array (splitmix64 seed 4), perft 1..depth through pb_perft (the
+    command line's loop) with `dtt_mb` MB of device tables and `htt_mb` MB of
+    host tables.  Seconds of the last depth for: the depth-first host driver
+    with the reference's always-overwrite replacement; two-slot size-priority
+    buckets; the breadth-first host driver with batched table-mode calls; and
+    the reference's own table build (oracle/_ref) with the same flags, as it
+    prints them.  Every count must agree."""
+    fen = pg.to_fen(pg.config_position(2, 4))
+    runs = {"depth_first_overwrite": {}, "depth_first_size_priority": {"tt_replace": 2},
+            f"breadth_first_ld{bf_launch_depth}_overwrite": {"host_driver": 2}}
+    out = {"workload": f"2 random plies (seed 4), perft {depth}, -dtt {dtt_mb} -htt {htt_mb}", "fen": fen,
+           "unit": "seconds of the last depth (host wall clock inside pb_perft)"}
+    counts = set()
+    for name, tun in runs.items():
+        ld = bf_launch_depth if tun.get("host_driver") == 2 else 0
+        eng = pg.Engine(device=0, use_tt=True, device_tt_mb=dtt_mb, host_tt_mb=htt_mb, launch_depth=ld)
+        if tun:
+            eng.set_tuning(**tun)
+        res = eng.perft(fen, depth)
+        eng.close()
+        counts.add(res[-1][0])
+        out[name] = {"seconds": res[-1][1], "seconds_all_depths": sum(s for _, s in res), "nodes": res[-1][0]}
+    if os.path.exists(REF_BIN):
+        txt = subprocess.run([REF_BIN, fen, str(depth), "-dtt", str(dtt_mb), "-htt", str(htt_mb)],
+                             capture_output=True, text=True, timeout=1200).stdout
+        lines = [l for l in txt.splitlines() if l.startswith("Perft(")]
+        if lines:
+            last = lines[-1]
+            n = int(last.split(":")[1].split(",")[0])
+            counts.add(n)
+            out["reference_tables"] = {"seconds": float(last.split("time:")[1].split("seconds")[0]), "nodes": n,
+                                       "seconds_all_depths": sum(float(l.split("time:")[1].split("seconds")[0])
+                                                                 for l in lines)}
+    assert len(counts) == 1, f"table runs disagree: {counts}"
+    return out
 
 
 def run_reference_arm(args):
@@ -330,6 +429,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the engine's default launch parameters")
     ap.add_argument("--no-positions", action="store_true", help="skip the batched-roots positions/s section")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's GPU build")
+    ap.add_argument("--no-tt", action="store_true", help="skip the deep table run (150 GB of device tables)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -466,12 +566,16 @@ def main():
                         "timing": "host wall clock around pb_perft_position"},
                 "gpu_launches": int(kernels), "clocks": clocks, "roofline": roofline}
         if world == 1 and not args.no_positions:
+            line["scheduler"] = scheduler_section(pg, eng)
             line["positions"] = positions_section(pg, eng, reps=min(args.steps, 3))
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(child_fens, depth)
             if cb:
                 line["cpu_baseline"] = cb
     eng.close()
+    if rank == 0 and world == 1 and not args.no_tt:
+        # after the engine released its memory: the tables take 150 GB
+        line["tt_run"] = tt_section(pg)
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         # after the engine released its memory; the reference allocates its own
         rg = reference_gpu(root_fen, depth)
