@@ -40,16 +40,6 @@ struct TTView {
 
 __device__ __forceinline__ u64 tt_slot(const TTView &t, u64 lo) { return __umul64hi(lo, t.slots); }
 
-// Does the shallow entry (w0, w1) hold key h?  (*count = its count)
-__device__ __forceinline__ bool tt_shallow_match(u64 w0, u64 w1, const Hash128 &h, u64 *count)
-{
-    if ((w0 ^ w1) == h.hi && ((w1 ^ (h.lo << 24)) & ~SHALLOW_COUNT_MASK) == 0 && (w1 & SHALLOW_COUNT_MASK)) {
-        *count = (w1 & SHALLOW_COUNT_MASK) - 1;
-        return true;
-    }
-    return false;
-}
-
 // Entry in slot `slot` matching the key?  (*count = its count; *used = slot holds anything)
 __device__ __forceinline__ bool tt_read(const TTView &t, u64 slot, const Hash128 &h, u64 *count, u64 *held)
 {
@@ -57,7 +47,11 @@ __device__ __forceinline__ bool tt_read(const TTView &t, u64 slot, const Hash128
         u64 w0, w1;
         asm volatile("ld.global.v2.u64 {%0,%1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(t.entries + 2 * slot));
         *held = (w1 & SHALLOW_COUNT_MASK) ? (w1 & SHALLOW_COUNT_MASK) - 1 : 0;
-        return tt_shallow_match(w0, w1, h, count);
+        if ((w0 ^ w1) == h.hi && ((w1 ^ (h.lo << 24)) & ~SHALLOW_COUNT_MASK) == 0 && (w1 & SHALLOW_COUNT_MASK)) {
+            *count = (w1 & SHALLOW_COUNT_MASK) - 1;
+            return true;
+        }
+        return false;
     }
     u64 w0, w1, w2, w3;
     asm volatile("ld.global.v4.u64 {%0,%1,%2,%3}, [%4];"
@@ -92,31 +86,6 @@ __device__ __forceinline__ bool tt_probe(const TTView &t, const Hash128 &h, u64 
     if (!t.buckets) return tt_read(t, slot, h, out, &held);
     slot &= ~1ULL;
     return tt_read(t, slot, h, out, &held) || tt_read(t, slot + 1, h, out, &held);
-}
-
-// A probe of a shallow table split in two, so the load can be issued long
-// before its result is needed: tt_fetch_shallow reads the key's slot (both
-// slots of its bucket with two-slot buckets, 32 contiguous bytes) and
-// tt_match_shallow compares afterwards.
-struct ShallowFetch {
-    u64 w[4];
-};
-__device__ __forceinline__ void tt_fetch_shallow(const TTView &t, const Hash128 &h, ShallowFetch &f)
-{
-    u64 slot = tt_slot(t, h.lo);
-    if (!t.buckets) {
-        asm volatile("ld.global.v2.u64 {%0,%1}, [%2];" : "=l"(f.w[0]), "=l"(f.w[1]) : "l"(t.entries + 2 * slot));
-        f.w[2] = f.w[3] = 0;
-        return;
-    }
-    slot &= ~1ULL;
-    asm volatile("ld.global.v4.u64 {%0,%1,%2,%3}, [%4];"
-                 : "=l"(f.w[0]), "=l"(f.w[1]), "=l"(f.w[2]), "=l"(f.w[3])
-                 : "l"(t.entries + 2 * slot));
-}
-__device__ __forceinline__ bool tt_match_shallow(const ShallowFetch &f, const Hash128 &h, u64 *count)
-{
-    return tt_shallow_match(f.w[0], f.w[1], h, count) || tt_shallow_match(f.w[2], f.w[3], h, count);
 }
 
 // Always-overwrite (the reference's rule, tt.h:60-70), or with two-slot
@@ -344,13 +313,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     Board b{};
     u32 st = 0;
     Hash128 h{};
-    const bool valid = i < n && pidx[i] < nparents;
-    // With SORT and the shallow leaf table, the probe's load is issued here
-    // and compared only after the ranking count, so its DRAM latency overlaps
-    // the count (a hit's count is then wasted: one count of its ~30).
-    const bool split_probe = SORT && tt.kind == TT_SHALLOW;
-    ShallowFetch f;
-    if (valid) {
+    if (i < n && pidx[i] < nparents) {
         u32 p = pidx[i];
         b = load_board(pboards + p);
         st = pstates[p];
@@ -359,9 +322,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
         make_move<C>(b, st, mv0);
         h = hash_move(phash[p], before, pstates[p], st, C, mv0);
         u64 hit;
-        if (split_probe)
-            tt_fetch_shallow(tt, h, f);
-        else if (tt_probe(tt, h, &hit))
+        if (tt_probe(tt, h, &hit))
             out[i] = (u32)hit;
         else
             miss = true;
@@ -372,20 +333,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
         __shared__ u32 s_i[PB_LEAF_THREADS];
         __shared__ uint8_t s_st[PB_LEAF_THREADS];
         __shared__ uint8_t s_key[PB_LEAF_THREADS];
-        u32 key;
-        if (split_probe) {
-            const u32 cnt = valid ? count_moves<1 - C, true>(b, st) : 0u;
-            u64 hit;
-            if (valid) {
-                if (tt_match_shallow(f, h, &hit))
-                    out[i] = (u32)hit;
-                else
-                    miss = true;
-            }
-            key = miss ? 1 + min(cnt, 254u) : 0u;
-        } else {
-            key = miss ? 1 + min(count_moves<1 - C, true>(b, st), 254u) : 0u;
-        }
+        const u32 key = miss ? 1 + min(count_moves<1 - C, true>(b, st), 254u) : 0u;
         const u32 rank = cta_rank_u8<PB_LEAF_THREADS>(key);
         s_b[rank] = b;
         s_h[rank] = h;
