@@ -1,7 +1,8 @@
 """Autotuner for the GPU path's launch parameters.
 
 Candidates: leaf kernel (one edge per thread / cooperative / one edge per
-thread with the CTA's children ranked by move count), the leaf's CTA size
+thread with the CTA's children ranked by move count / ranked with each
+child's own-piece squares listed once), the leaf's CTA size
 (128/256/512), the staged generator's CTA size and tile (64 or 128
 threads, 64 moves staged per thread) and the leaf fuse depth (two plies fused
 in the leaf, or one with an extra BFS level).  Each candidate runs perft 7
@@ -42,8 +43,9 @@ def candidates() -> List[Dict[str, int]]:
     for lt, gt, fuse in itertools.product((128, 256, 512), (64, 128), (2, 1)):
         out.append({"leaf_kernel": 1, "leaf_threads": lt, "gen_threads": gt, "leaf_fuse": fuse})
     out.append({"leaf_kernel": 2, "leaf_threads": 256, "gen_threads": 128, "leaf_fuse": 2})
-    for gt in (64, 128):
-        out.append({"leaf_kernel": 4, "leaf_threads": 256, "gen_threads": gt, "leaf_fuse": 2})
+    for lk in (4, 5):
+        for gt in (64, 128):
+            out.append({"leaf_kernel": lk, "leaf_threads": 256, "gen_threads": gt, "leaf_fuse": 2})
     return out
 
 

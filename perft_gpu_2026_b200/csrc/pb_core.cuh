@@ -290,7 +290,7 @@ struct BitboardPieces {
     }
 };
 
-// ListedPieces serves the positions one move of the OTHER side away from a
+// Listed pieces serve the positions one move of the OTHER side away from a
 // position P (the grandchildren of the fused leaf): the side to move there has
 // the pieces it had in P, less at most one that the other side captured.  Its
 // knight, diagonal-mover (bishop, queen) and orthogonal-mover (rook, queen)
@@ -298,17 +298,20 @@ struct BitboardPieces {
 // (square + 1, 0 = end), so the counts iterate the lists instead of scanning
 // bitboards.  Pieces whose move set differs from the plain one (captured, or
 // pinned) are corrected afterwards; that path is rare.
+//
+// ListedPieces::build writes the three lists and the listed squares to
+// caller storage (shared memory in the leaf kernels: kept in registers across
+// the grandchild loop they made the kernel spill); ListedView is the counting
+// policy that reads them back at every count.
 struct ListedPieces {
-    u32 kn = 0, dg = 0, og = 0;
-    u64 listed = 0;  // squares in the lists
-
-    // Lists side C's pieces of `b`; false if a kind has more than four.
-    template <int C> PB_HD bool build(const Board &b)
+    // Lists side C's pieces of `b` into l[0..2] and *listed; false if a kind
+    // has more than four.
+    template <int C> static PB_HD bool build(const Board &b, u32 *l, u64 *listed)
     {
         Sets s = derive<C>(b);
         u64 k = s.knights & s.us, d = s.bq & s.us, o = s.rq & s.us;
-        listed = k | d | o;
-        return pack(k, kn) && pack(d, dg) && pack(o, og);
+        *listed = k | d | o;
+        return pack(k, l[0]) && pack(d, l[1]) && pack(o, l[2]);
     }
     static PB_HD bool pack(u64 set, u32 &out)
     {
@@ -326,25 +329,31 @@ struct ListedPieces {
         u32 x = list ^ (key * 0x01010101u);
         return ((x - 0x01010101u) & ~x & 0x80808080u) != 0;
     }
+};
+
+struct ListedView {
+    const volatile u32 *l;  // knights, diagonal movers, orthogonal movers
+    const volatile u64 *m;  // the listed squares
     PB_HD u32 count(const Sets &s, u64 movable, u64 targets, u64 pinned_lines, int ksq) const
     {
+        const u32 kn = l[0], dg = l[1], og = l[2];
         u32 n = 0;
-        for (u32 l = kn; l; l >>= 8) n += popc(knight_att((int)(l & 255) - 1) & targets);
-        for (u32 l = dg; l; l >>= 8) n += popc(bishop_att((int)(l & 255) - 1, s.occ) & targets);
-        for (u32 l = og; l; l >>= 8) n += popc(rook_att((int)(l & 255) - 1, s.occ) & targets);
+        for (u32 q = kn; q; q >>= 8) n += popc(knight_att((int)(q & 255) - 1) & targets);
+        for (u32 q = dg; q; q >>= 8) n += popc(bishop_att((int)(q & 255) - 1, s.occ) & targets);
+        for (u32 q = og; q; q >>= 8) n += popc(rook_att((int)(q & 255) - 1, s.occ) & targets);
         // listed squares that are not movable: captured (no longer own) or
         // pinned.  Take back what the lists counted for them and add the
         // pinned sliders' moves along their lines.
-        for (u64 fix = listed & ~movable; fix; fix &= fix - 1) {
+        for (u64 fix = *m & ~movable; fix; fix &= fix - 1) {
             const int sq = lsb(fix);
             const u32 key = (u32)sq + 1;
             const u64 line = ((pinned_lines & s.us) >> sq) & 1 ? line_through(sq, ksq) : 0;
-            if (has(kn, key)) n -= popc(knight_att(sq) & targets);
-            if (has(dg, key)) {
+            if (ListedPieces::has(kn, key)) n -= popc(knight_att(sq) & targets);
+            if (ListedPieces::has(dg, key)) {
                 u64 a = bishop_att(sq, s.occ);
                 n += popc(a & ~s.us & line) - popc(a & targets);
             }
-            if (has(og, key)) {
+            if (ListedPieces::has(og, key)) {
                 u64 a = rook_att(sq, s.occ);
                 n += popc(a & ~s.us & line) - popc(a & targets);
             }

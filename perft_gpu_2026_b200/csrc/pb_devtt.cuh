@@ -296,12 +296,13 @@ __global__ void k_dedup_resolve(const Hash128 *__restrict__ h, uint8_t *__restri
     }
 }
 
-// Leaf with the depth-2 table: perft 2 of each edge's child, per edge.  With
-// SORT (blockDim.x must be PB_LEAF_THREADS) table hits are answered first and
+// Leaf with the depth-2 table: perft 2 of each edge's child, per edge.  MODE
+// is the leaf mode of grandchild_counts.  With MODE >= 1 (blockDim.x must be
+// PB_LEAF_THREADS) table hits are answered first and
 // the CTA's misses are ranked by move count and handed to threads in that
 // order, so the misses fill whole warps (all-hit warps then have no work) and
 // each warp's misses have similar loop lengths.
-template <int C, bool STRICT, bool SORT = false>
+template <int C, bool STRICT, int MODE = 0>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_tt(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                const Hash128 *__restrict__ phash, const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
         else
             miss = true;
     }
-    if (SORT) {
+    if (MODE >= 1) {
         __shared__ Board s_b[PB_LEAF_THREADS];
         __shared__ Hash128 s_h[PB_LEAF_THREADS];
         __shared__ u32 s_i[PB_LEAF_THREADS];
@@ -351,12 +352,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
         uint16_t mv[MAX_MOVES];
         ArraySink sink{mv, 0};
         gen_moves<1 - C>(b, st, sink);
-        for (int k = 0; k < sink.n; k++) {
-            Board g = b;
-            u32 gs = st;
-            make_move<1 - C>(g, gs, mv[k]);
-            total += count_moves<C, STRICT>(g, gs);
-        }
+        total = grandchild_counts<C, STRICT, MODE == 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
         counted = sink.n;
         tt_store(tt, h, total);
         out[i] = total;

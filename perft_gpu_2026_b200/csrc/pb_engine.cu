@@ -40,7 +40,7 @@ struct GraphPlan {
     u64 n = 0;
     int depth = 0;
     bool strict = false;
-    bool sort = false;   // leaf ranks each CTA's children by move count
+    int mode = 0;        // leaf mode (leaf_mode)
     bool queue = false;  // persistent work-queue leaf instead of the grid leaf
     std::vector<u64> caps;
     cudaGraphExec_t exec = nullptr;
@@ -50,9 +50,9 @@ struct GraphPlan {
     u32 *r0 = nullptr;
     unsigned long long *rc = nullptr;
     u64 *sizes = nullptr;
-    bool same(u64 n_, int d_, bool s_, bool sort_, bool queue_, const std::vector<u64> &c_) const
+    bool same(u64 n_, int d_, bool s_, int mode_, bool queue_, const std::vector<u64> &c_) const
     {
-        return exec && n == n_ && depth == d_ && strict == s_ && sort == sort_ && queue == queue_ && caps == c_;
+        return exec && n == n_ && depth == d_ && strict == s_ && mode == mode_ && queue == queue_ && caps == c_;
     }
 };
 
@@ -178,6 +178,13 @@ struct Arena {
 };
 
 inline unsigned grid_for(u64 n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+// Leaf mode of the batched, planned and table leaves (grandchild_counts):
+// 2 for leaf kernel 5 (ranked, listed pieces), 1 for 4 (ranked), else 0.
+inline int leaf_mode(const pb_ctx *ctx)
+{
+    return ctx->tuning.leaf_kernel == 5 ? 2 : ctx->tuning.leaf_kernel == 4 ? 1 : 0;
+}
 
 // NVTX range for profilers (header-only NVTX v3: free unless a tool attaches):
 // marks each BFS pass, level and leaf launch on the host timeline, so a
@@ -626,14 +633,17 @@ int bfs_tt_roots(pb_ctx *ctx, const Board *rb, const uint8_t *rs, const Hash128 
     if (n > 0) {
         TTView tv = ctx->dtt.at(2);
         unsigned g = grid_for(n, PB_LEAF_THREADS);
-        const bool sort = ctx->tuning.leaf_kernel >= 4;
+        const int mode = leaf_mode(ctx);
 #define PB_TT_LEAF(CC, SS)                                                                                     \
-    if (sort)                                                                                                  \
-        k_leaf2_tt<CC, SS, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,     \
-                                                               leafcnt, ctx->d_counter);                      \
+    if (mode == 2)                                                                                             \
+        k_leaf2_tt<CC, SS, 2><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,        \
+                                                            leafcnt, ctx->d_counter);                         \
+    else if (mode == 1)                                                                                        \
+        k_leaf2_tt<CC, SS, 1><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,        \
+                                                            leafcnt, ctx->d_counter);                         \
     else                                                                                                       \
-        k_leaf2_tt<CC, SS, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,    \
-                                                                leafcnt, ctx->d_counter);
+        k_leaf2_tt<CC, SS, 0><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,        \
+                                                            leafcnt, ctx->d_counter);
         if (c == WHITE) {
             if (strict) {
                 PB_TT_LEAF(WHITE, true)
@@ -900,14 +910,17 @@ int bfs_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth,
             }
         } else {
             unsigned g = grid_for(ne, PB_LEAF_THREADS);
-            const bool sort = ctx->tuning.leaf_kernel >= 4;
+            const int mode = leaf_mode(ctx);
 #define PB_ROOTED_LEAF(CC, SS)                                                                                   \
-    if (sort)                                                                                                    \
-        k_leaf2_rooted<CC, SS, true><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, \
-                                                                   ctx->d_counter);                              \
+    if (mode == 2)                                                                                               \
+        k_leaf2_rooted<CC, SS, 2><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc,    \
+                                                                ctx->d_counter);                                 \
+    else if (mode == 1)                                                                                          \
+        k_leaf2_rooted<CC, SS, 1><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc,    \
+                                                                ctx->d_counter);                                 \
     else                                                                                                         \
-        k_leaf2_rooted<CC, SS, false><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc, \
-                                                                    ctx->d_counter);
+        k_leaf2_rooted<CC, SS, 0><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc,    \
+                                                                ctx->d_counter);
             if (c == WHITE) {
                 if (strict) {
                     PB_ROOTED_LEAF(WHITE, true)
@@ -984,46 +997,56 @@ struct GraphLevel {
     u64 tiles;
 };
 
-template <int C, bool S, bool SORT>
+template <int C, bool S, int MODE>
 void launch_leaf_queue_t(cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r, const u32 *pi,
                          const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev, u64 npar_cap,
                          unsigned long long *cursor, unsigned long long *rc, unsigned long long *counter, u32 *err)
 {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf2_rooted_queue<C, S, SORT>, PB_LEAF_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf2_rooted_queue<C, S, MODE>, PB_LEAF_THREADS, 0);
     if (per_sm <= 0) per_sm = 1;
     unsigned grid = (unsigned)std::min<u64>((u64)sms * per_sm, (cap + PB_LEAF_THREADS - 1) / PB_LEAF_THREADS + 1);
-    k_leaf2_rooted_queue<C, S, SORT><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev,
+    k_leaf2_rooted_queue<C, S, MODE><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev,
                                                                       npar_cap, cursor, rc, counter, err);
 }
-template <int C, bool S, bool SORT>
+template <int C, bool S, int MODE>
 void launch_leaf_grid_t(cudaStream_t s, const Board *b, const uint8_t *st, const u32 *r, const u32 *pi,
                         const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev, u64 npar_cap,
                         unsigned long long *rc, unsigned long long *counter, u32 *err)
 {
     unsigned grid = (unsigned)std::max<u64>((cap + PB_LEAF_THREADS - 1) / PB_LEAF_THREADS, 1);
-    k_leaf2_rooted_dev<C, S, SORT><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap,
+    k_leaf2_rooted_dev<C, S, MODE><<<grid, PB_LEAF_THREADS, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap,
                                                                     rc, counter, err);
 }
 // Leaf of a planned batch: the grid leaf over the planned capacity, or the
 // persistent work-queue leaf (queue).
+template <int C, bool S, int MODE>
+void launch_leaf_planned_t(bool queue, cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r,
+                           const u32 *pi, const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev,
+                           u64 npar_cap, unsigned long long *cursor, unsigned long long *rc,
+                           unsigned long long *counter, u32 *err)
+{
+    if (queue)
+        launch_leaf_queue_t<C, S, MODE>(s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc, counter,
+                                        err);
+    else
+        launch_leaf_grid_t<C, S, MODE>(s, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, rc, counter, err);
+}
 template <int C, bool S>
-void launch_leaf_queue(bool sort, bool queue, cudaStream_t s, int sms, const Board *b, const uint8_t *st,
+void launch_leaf_queue(int mode, bool queue, cudaStream_t s, int sms, const Board *b, const uint8_t *st,
                        const u32 *r, const u32 *pi, const uint16_t *mv, const u64 *n_dev, u64 cap,
                        const u64 *npar_dev, u64 npar_cap, unsigned long long *cursor, unsigned long long *rc,
                        unsigned long long *counter, u32 *err)
 {
-    if (!queue) {
-        if (sort)
-            launch_leaf_grid_t<C, S, true>(s, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, rc, counter, err);
-        else
-            launch_leaf_grid_t<C, S, false>(s, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, rc, counter, err);
-        return;
-    }
-    if (sort)
-        launch_leaf_queue_t<C, S, true>(s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc, counter, err);
+    if (mode == 2)
+        launch_leaf_planned_t<C, S, 2>(queue, s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc,
+                                       counter, err);
+    else if (mode == 1)
+        launch_leaf_planned_t<C, S, 1>(queue, s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc,
+                                       counter, err);
     else
-        launch_leaf_queue_t<C, S, false>(s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc, counter, err);
+        launch_leaf_planned_t<C, S, 0>(queue, s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc,
+                                       counter, err);
 }
 
 // Builds (captures) the graph for a planned batch shape.
@@ -1133,17 +1156,17 @@ int capture_batch_graph(pb_ctx *ctx, GraphPlan &g)
                                                                 npar_cap, g.rc, ctx->d_err);
     } else if (c == WHITE) {
         if (g.strict)
-            launch_leaf_queue<WHITE, true>(g.sort, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
+            launch_leaf_queue<WHITE, true>(g.mode, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
                                            npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
         else
-            launch_leaf_queue<WHITE, false>(g.sort, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
+            launch_leaf_queue<WHITE, false>(g.mode, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
                                             npar, npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
     } else {
         if (g.strict)
-            launch_leaf_queue<BLACK, true>(g.sort, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
+            launch_leaf_queue<BLACK, true>(g.mode, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap, npar,
                                            npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
         else
-            launch_leaf_queue<BLACK, false>(g.sort, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
+            launch_leaf_queue<BLACK, false>(g.mode, g.queue, s, ctx->num_sms, pb_, ps, pr, L[nlev].pi, L[nlev].mv, d_n0 + nlev, lcap,
                                             npar, npar_cap, cursor, g.rc, ctx->d_counter, ctx->d_err);
     }
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
@@ -1164,13 +1187,13 @@ int run_planned_batch(pb_ctx *ctx, GraphPlan &g, const Board *rb, const uint8_t 
     NvtxRange nvtx_pass("planned_batch");
     *overflow = false;
     const bool strict = ctx->opts.strict != 0;
-    const bool sort = ctx->tuning.leaf_kernel >= 4;
+    const int mode = leaf_mode(ctx);
     const bool queue = ctx->tuning.planned_leaf == 2;
-    if (!g.same(n, depth, strict, sort, queue, caps)) {
+    if (!g.same(n, depth, strict, mode, queue, caps)) {
         g.n = n;
         g.depth = depth;
         g.strict = strict;
-        g.sort = sort;
+        g.mode = mode;
         g.queue = queue;
         g.caps = caps;
         int rc = capture_batch_graph(ctx, g);
@@ -1613,9 +1636,11 @@ template <int Z>
 u64 check_listed_t(const Board &y, u32 ys, u64 *checked)
 {
     constexpr int C = 1 - Z;
-    ListedPieces own;
+    u32 lists[3];
+    u64 listed;
     *checked = 0;
-    if (!own.build<C>(y)) return 0;
+    if (!ListedPieces::build<C>(y, lists, &listed)) return 0;
+    const ListedView own{lists, &listed};
     uint16_t mv[MAX_MOVES];
     ArraySink sink{mv, 0};
     gen_moves<Z>(y, ys, sink);

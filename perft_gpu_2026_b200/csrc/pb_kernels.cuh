@@ -324,6 +324,42 @@ __global__ void __launch_bounds__(GT) k_generate(const Board *__restrict__ board
 }
 
 // ---------------------------------------------------------------- leaves
+// Sum over the moves mv[0..n) of child b of their grandchildren's move counts
+// (each move made on a copy of b, then counted).  With LISTED the counts
+// iterate the child's own-piece lists (ListedPieces, read back through
+// ListedView from this thread's slot of a shared-memory array of T slots); a
+// child with more than four pieces of one kind counts with bitboard scans.
+// Leaf modes of the ranked leaves: 0 = unranked, 1 = the CTA's children
+// ranked by move count, 2 = ranked and counted with listed pieces.
+template <int C, bool STRICT, bool LISTED, int T>
+__device__ __forceinline__ u32 grandchild_counts(const Board &b, u32 st, const uint16_t *mv, int n)
+{
+    u32 total = 0;
+    if (LISTED) {
+        __shared__ u32 s_lists[T][3];
+        __shared__ u64 s_listed[T];
+        u32 *l = s_lists[threadIdx.x];
+        u64 *m = &s_listed[threadIdx.x];
+        if (ListedPieces::build<C>(b, l, m)) {
+            const ListedView own{l, m};
+            for (int k = 0; k < n; k++) {
+                Board g = b;
+                u32 gs = st;
+                make_move<1 - C>(g, gs, mv[k]);
+                total += count_moves<C, STRICT>(g, gs, own);
+            }
+            return total;
+        }
+    }
+    for (int k = 0; k < n; k++) {
+        Board g = b;
+        u32 gs = st;
+        make_move<1 - C>(g, gs, mv[k]);
+        total += count_moves<C, STRICT>(g, gs);
+    }
+    return total;
+}
+
 // One-ply leaf: the move count of each edge's child (perft 1 of the child).
 template <int C, bool STRICT>
 __global__ void __launch_bounds__(256) k_leaf1(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
@@ -507,7 +543,9 @@ __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_sorted(const Board *__res
 // of a child has the pieces of side C that the child has, less at most one
 // captured piece, so the knight and slider squares are listed once per child.
 // A child with more than four pieces of one kind counts with the bitboard
-// scans.  Same counts as k_leaf2_sorted.
+// scans.  Same counts as k_leaf2_sorted.  Measured on B200 (perft 7 of the
+// bench position): 21.16 ms against 21.97 ms for k_leaf2_sorted, 21.38 ms
+// with the lists held in registers (which spilled).
 template <int C, bool STRICT, int T>
 __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_listed(const Board *__restrict__ pboards,
                                                               const uint8_t *__restrict__ pstates,
@@ -541,22 +579,7 @@ __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_listed(const Board *__res
         uint16_t mv[MAX_MOVES];
         ArraySink sink{mv, 0};
         gen_moves<1 - C>(b, st, sink);
-        ListedPieces own;
-        if (own.build<C>(b)) {
-            for (int k = 0; k < sink.n; k++) {
-                Board g = b;
-                u32 gs = st;
-                make_move<1 - C>(g, gs, mv[k]);
-                total += count_moves<C, STRICT>(g, gs, own);
-            }
-        } else {
-            for (int k = 0; k < sink.n; k++) {
-                Board g = b;
-                u32 gs = st;
-                make_move<1 - C>(g, gs, mv[k]);
-                total += count_moves<C, STRICT>(g, gs);
-            }
-        }
+        total = grandchild_counts<C, STRICT, true, T>(b, st, mv, sink.n);
         counted = sink.n;
     }
     total = __reduce_add_sync(0xffffffffu, total);
@@ -781,10 +804,10 @@ __device__ __forceinline__ void rank_children(Board &b, u32 &st, u32 &root, bool
     __syncthreads();  // the exchange arrays are free again
 }
 
-// Two-ply leaf over edges, counts credited to each edge's root.  With SORT
-// the CTA's children are ranked by move count first (blockDim.x must be
-// PB_LEAF_THREADS).
-template <int C, bool STRICT, bool SORT>
+// Two-ply leaf over edges, counts credited to each edge's root.  MODE is the
+// leaf mode of grandchild_counts: with 1 or 2 the CTA's children are ranked
+// by move count first (blockDim.x must be PB_LEAF_THREADS).
+template <int C, bool STRICT, int MODE>
 __device__ __forceinline__ void leaf2_rooted_cta(const Board *__restrict__ pboards,
                                                  const uint8_t *__restrict__ pstates, const u32 *__restrict__ proot,
                                                  const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
@@ -803,17 +826,12 @@ __device__ __forceinline__ void leaf2_rooted_cta(const Board *__restrict__ pboar
         st = pstates[p];
         make_move<C>(b, st, moves[i]);
     }
-    if (SORT) rank_children<C, PB_LEAF_THREADS>(b, st, root, valid);
+    if (MODE >= 1) rank_children<C, PB_LEAF_THREADS>(b, st, root, valid);
     if (valid) {
         uint16_t mv[MAX_MOVES];
         ArraySink sink{mv, 0};
         gen_moves<1 - C>(b, st, sink);
-        for (int k = 0; k < sink.n; k++) {
-            Board g = b;
-            u32 gs = st;
-            make_move<1 - C>(g, gs, mv[k]);
-            total += count_moves<C, STRICT>(g, gs);
-        }
+        total = grandchild_counts<C, STRICT, MODE == 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
         counted = sink.n;
     }
     add_by_key(root_counts, root, total, valid);
@@ -821,14 +839,14 @@ __device__ __forceinline__ void leaf2_rooted_cta(const Board *__restrict__ pboar
     if ((threadIdx.x & 31) == 0 && counted) atomicAdd(counter + 1, (unsigned long long)counted);
 }
 
-template <int C, bool STRICT, bool SORT = false>
+template <int C, bool STRICT, int MODE = 0>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_rooted(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                    const u32 *__restrict__ proot, const u32 *__restrict__ pidx, const uint16_t *__restrict__ moves,
                    u64 n, u64 nparents, unsigned long long *__restrict__ root_counts,
                    unsigned long long *__restrict__ counter)
 {
-    leaf2_rooted_cta<C, STRICT, SORT>(pboards, pstates, proot, pidx, moves, n, nparents, root_counts, counter);
+    leaf2_rooted_cta<C, STRICT, MODE>(pboards, pstates, proot, pidx, moves, n, nparents, root_counts, counter);
 }
 
 // One-ply leaf over edges (perft 1 of each edge's child), per root.
@@ -880,7 +898,7 @@ __device__ __forceinline__ u64 dev_size(const u64 *n_dev, u64 cap, u32 *err)
 // the grid covers the planned capacity and the CTAs past the level's actual
 // size leave at once (a whole CTA at a time, so the ranking's barriers are
 // reached by all of its threads or by none).
-template <int C, bool STRICT, bool SORT = false>
+template <int C, bool STRICT, int MODE = 0>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_rooted_dev(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                        const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
@@ -891,7 +909,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     const u64 n = dev_size(n_dev, cap, err);
     if ((u64)blockIdx.x * blockDim.x >= n) return;
     const u64 npar = min(*npar_dev, npar_cap);
-    leaf2_rooted_cta<C, STRICT, SORT>(pboards, pstates, proot, pidx, moves, n, npar, root_counts, counter);
+    leaf2_rooted_cta<C, STRICT, MODE>(pboards, pstates, proot, pidx, moves, n, npar, root_counts, counter);
 }
 
 // Scan with a device-resident length (grid = tiles of the capacity; surplus
@@ -1006,7 +1024,7 @@ __global__ void __launch_bounds__(256) k_expand_rooted_dev(const Board *__restri
 // grid.  The grab is per CTA, not per warp: the CTA's warps then work on
 // sibling edges whose attack-table lines they share in L1 (per-warp grabs of
 // 32, 64 or 128 edges measured 2.6-6 % slower on B200).
-template <int C, bool STRICT, bool SORT = false>
+template <int C, bool STRICT, int MODE = 0>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_rooted_queue(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
                          const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
@@ -1038,17 +1056,12 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
             st = pstates[p];
             make_move<C>(b, st, moves[i]);
         }
-        if (SORT) rank_children<C, PB_LEAF_THREADS>(b, st, root, valid);
+        if (MODE >= 1) rank_children<C, PB_LEAF_THREADS>(b, st, root, valid);
         if (valid) {
             uint16_t mv[MAX_MOVES];
             ArraySink sink{mv, 0};
             gen_moves<1 - C>(b, st, sink);
-            for (int k = 0; k < sink.n; k++) {
-                Board g = b;
-                u32 gs = st;
-                make_move<1 - C>(g, gs, mv[k]);
-                total += count_moves<C, STRICT>(g, gs);
-            }
+            total = grandchild_counts<C, STRICT, MODE == 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
             counted += sink.n;
         }
         add_by_key(root_counts, root, total, valid);

@@ -248,7 +248,9 @@ def test_edge_depths_and_terminal_positions(gpu_engine, oracle):
 
 def test_batched_leaf_ranked_and_unranked_agree():
     """The batched leaf with and without ranking each CTA's children by move
-    count (leaf_kernel 4 / 1), on uneven roots, both colours to move."""
+    count, and ranked with listed pieces (leaf_kernel 4 / 1 / 5), on uneven
+    roots, both colours to move; also the planned batches' grid and queue
+    leaves with listed pieces."""
     eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
     roots = pg.uneven_roots(192, 6, 40, seed=23)
     depths = [2 + (i % 4) for i in range(len(roots))]
@@ -256,8 +258,15 @@ def test_batched_leaf_ranked_and_unranked_agree():
     ranked = eng.perft_batch(roots, depths)
     eng.set_tuning(leaf_kernel=1)
     plain = eng.perft_batch(roots, depths)
-    assert ranked == plain
+    eng.set_tuning(leaf_kernel=5)
+    listed = eng.perft_batch(roots, depths)
+    assert ranked == plain == listed
     assert ranked == [eng.perft_position(r, d) for r, d in zip(roots, depths)]
+    eng.mlp_init(seed=3, out_bias=[4.5, 9.5, 14.5, 19.0])
+    for planned_leaf in (1, 2):
+        eng.set_tuning(planned_leaf=planned_leaf)
+        got, _ = eng.perft_batch_planned(roots, depths)
+        assert list(got) == ranked, planned_leaf
     eng.close()
 
 

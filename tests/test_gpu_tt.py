@@ -112,3 +112,21 @@ def test_breadth_first_host_driver_on_the_gpu(use_tt):
         assert got == ref.perft_position(p, 7)
     ref.close()
     eng.close()
+
+
+@pytest.mark.parametrize("leaf_kernel", [1, 5])
+def test_table_leaf_modes_match_fixtures(golden, leaf_kernel):
+    """The table leaf unranked (leaf kernel 1) and ranked with listed pieces
+    (5) against the reference fixtures and the bench position."""
+    eng = pg.Engine(device=0, use_tt=True, arena_bytes=2 << 30, device_tt_mb=1024, host_tt_mb=256)
+    eng.set_tuning(leaf_kernel=leaf_kernel)
+    bad = []
+    for case in golden:
+        p = pg.parse_fen(case["fen"])
+        for d, want in enumerate(case["counts"], start=1):
+            got = eng.perft_position(p, d)
+            if got != want:
+                bad.append((case["name"], d, got, want))
+    assert not bad, bad
+    assert eng.perft_position(pg.config_position(4, 1), 7) == 26402736244
+    eng.close()
