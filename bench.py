@@ -542,8 +542,13 @@ def main():
                     "positions_per_s": leaf_pos / (my_leaf_ms / 1e3) if my_leaf_ms > 0 else None,
                     "achieved": None, "frac": None,
                     "traffic": dram_per_pos * leaf_pos if dram_per_pos else None,
-                    "traffic_note": "DRAM bytes per move-count call from the committed ncu capture "
-                                    "(profiles/), scaled by this launch's calls"}
+                    "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum per move-count call, "
+                                    "from the ncu capture of this kernel's depth-7 launch of this position "
+                                    "(profiles/), times this launch's calls",
+                    "algorithmic_bytes": consts.get("algorithmic_bytes_per_launch"),
+                    "algorithmic_note": "the leaf's compulsory DRAM reads: 6 B per edge (move, parent index) "
+                                        "and 33 B per parent position; the leaf is bound by integer issue, "
+                                        "not by these bytes"}
         if inst_per_pos:
             ach = inst_per_pos * leaf_pos / (my_leaf_ms / 1e3) / 1e9
             roofline["achieved"] = ach
@@ -554,7 +559,8 @@ def main():
             # rate, so the issue fraction cannot reach 1 with this mix
             roofline["binding_unit"] = {"unit": "ALU pipe", "util_pct": consts["ncu_alu_pipe_pct"],
                                         "issue_active_pct": consts.get("ncu_issue_active_pct"),
-                                        "source": "ncu --set full capture of the same kernel (profiles/)"}
+                                        "source": consts.get("pipe_source",
+                                                             "ncu --set full capture of the same kernel (profiles/)")}
         line = {"metric": METRIC, "value": nodes / (my_ms / 1e3), "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": my_ms, "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
