@@ -90,8 +90,10 @@ def test_trained_network_plans_a_tight_arena_better_than_a_constant_guess():
         assert got == want, name
         res[name] = (mae, st.retries)
     eng.close()
+    # a strict gain: the constant guess must rerun at least one batch, the
+    # trained network none
     assert res["trained"][1] == 0, res
-    assert res["constant"][1] >= res["trained"][1], res
+    assert res["constant"][1] > res["trained"][1], res
     assert res["trained"][0] < 0.8 * res["constant"][0], res
 
 
