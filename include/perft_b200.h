@@ -179,9 +179,9 @@ typedef struct {
  * Zero fields keep the current value.  leaf_kernel: 1 = one edge per thread,
  * 2 = cooperative (grandchildren spread over the CTA), 3 = in-check children
  * deferred to a second pass, 4 = one edge per thread with the CTA's children
- * ranked by move count first (default), 5 = as 4 with each child's own-piece
- * squares listed once for all of its grandchild counts (batched, planned and
- * table leaves rank their children for 4 and 5);
+ * ranked by move count first, 5 = as 4 with each child's own-piece squares
+ * listed once for all of its grandchild counts (default; batched, planned and
+ * table leaves rank their children for 4 and 5 and list pieces for 5);
  * leaf_blocks_per_sm: persistent grid of the cooperative leaf. */
 typedef struct {
     int leaf_kernel;

@@ -546,8 +546,11 @@ __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_sorted(const Board *__res
 // scans.  Same counts as k_leaf2_sorted.  Measured on B200 (perft 7 of the
 // bench position): 21.16 ms against 21.97 ms for k_leaf2_sorted, 21.38 ms
 // with the lists held in registers (which spilled).
+#ifndef PB_LISTED_WARPS_PER_SM
+#define PB_LISTED_WARPS_PER_SM 32  // resident warps the listed leaf is compiled for (64 registers)
+#endif
 template <int C, bool STRICT, int T>
-__global__ void __launch_bounds__(T, 1024 / T) k_leaf2_listed(const Board *__restrict__ pboards,
+__global__ void __launch_bounds__(T, PB_LISTED_WARPS_PER_SM * 32 / T) k_leaf2_listed(const Board *__restrict__ pboards,
                                                               const uint8_t *__restrict__ pstates,
                                                               const u32 *__restrict__ pidx,
                                                               const uint16_t *__restrict__ moves, u64 n, u64 nparents,

@@ -2,7 +2,7 @@
 capture ends by itself.  The summaries under profiles/ name the command line
 that produced them.
 
-    python profile_workloads.py leaf   [--depth 7] [--arena-gb 2] [--reps 3]
+    python profile_workloads.py leaf   [--depth 7] [--arena-gb 2] [--reps 3] [--leaf-kernel K] [--leaf-threads T]
     python profile_workloads.py levels [--roots 16384] [--depth 5] [--arena-gb 6]
     python profile_workloads.py tt     [--depth 8] [--dtt-mb 2000] [--arena-gb 2]
 
@@ -33,8 +33,8 @@ START_TOTALS = {5: 4865609, 6: 119060324, 7: 3195901860, 8: 84998978956, 9: 2439
 
 def leaf(args):
     eng = pg.Engine(device=0, use_tt=False, arena_bytes=args.arena_gb << 30)
-    if args.leaf_kernel:
-        eng.set_tuning(leaf_kernel=args.leaf_kernel)
+    if args.leaf_kernel or args.leaf_threads:
+        eng.set_tuning(leaf_kernel=args.leaf_kernel, leaf_threads=args.leaf_threads)
     eng.set_timing(True)
     root = pg.config_position(4, 1)
     out = None
@@ -45,7 +45,7 @@ def leaf(args):
             raise SystemExit("count changed between passes")
         out = {"workload": "leaf", "depth": args.depth, "nodes": got, "device_ms": st.device_ms,
                "leaf_ms": st.leaf_ms, "leaf_edges": st.leaf_edges, "leaf_positions": st.leaf_positions,
-               "leaf_kernel": eng.get_tuning().leaf_kernel}
+               "leaf_kernel": eng.get_tuning().leaf_kernel, "leaf_threads": eng.get_tuning().leaf_threads}
     print(json.dumps(out))
     eng.close()
 
@@ -90,6 +90,7 @@ def main(argv=None):
     a.add_argument("--arena-gb", type=int, default=2)
     a.add_argument("--reps", type=int, default=3)
     a.add_argument("--leaf-kernel", type=int, default=0)
+    a.add_argument("--leaf-threads", type=int, default=0)
     a = sub.add_parser("levels")
     a.add_argument("--roots", type=int, default=1 << 14)
     a.add_argument("--depth", type=int, default=5)
