@@ -87,11 +87,12 @@ class Tuning(ctypes.Structure):
 
     _fields_ = [("leaf_kernel", ctypes.c_int), ("leaf_blocks_per_sm", ctypes.c_int),
                 ("leaf_threads", ctypes.c_int), ("gen_threads", ctypes.c_int), ("leaf_fuse", ctypes.c_int),
-                ("tt_replace", ctypes.c_int), ("planned_leaf", ctypes.c_int), ("host_driver", ctypes.c_int)]
+                ("tt_replace", ctypes.c_int), ("planned_leaf", ctypes.c_int), ("host_driver", ctypes.c_int),
+                ("tt_leaf", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k in ("leaf_kernel", "leaf_blocks_per_sm", "leaf_threads", "gen_threads",
-                                              "leaf_fuse", "tt_replace", "planned_leaf", "host_driver")}
+                                              "leaf_fuse", "tt_replace", "planned_leaf", "host_driver", "tt_leaf")}
 
 
 class PlanStats(ctypes.Structure):
@@ -429,7 +430,7 @@ class Engine:
 
     def set_tuning(self, leaf_kernel: int = 0, leaf_blocks_per_sm: int = 0, leaf_threads: int = 0,
                    gen_threads: int = 0, leaf_fuse: int = 0, tt_replace: int = 0, planned_leaf: int = 0,
-                   host_driver: int = 0) -> None:
+                   host_driver: int = 0, tt_leaf: int = 0) -> None:
         """Launch parameters (pb_set_tuning); 0 keeps the current value.
         leaf_kernel 1 = one edge per thread, 2 = cooperative, 3 = in-check
         children deferred, 4 = children ranked by move count,
@@ -439,11 +440,13 @@ class Engine:
         planned_leaf 1 = grid over the planned capacity (default),
         2 = persistent work-queue leaf; host_driver 1 = depth-first tree
         above the launch depth (default), 2 = breadth first with batched
-        GPU calls."""
+        GPU calls; tt_leaf 1 = one edge per thread, 2 = persistent table leaf
+        that counts only full CTAs of table misses."""
         t = Tuning()
         t.tt_replace = tt_replace
         t.planned_leaf = planned_leaf
         t.host_driver = host_driver
+        t.tt_leaf = tt_leaf
         t.leaf_kernel = leaf_kernel
         t.leaf_blocks_per_sm = leaf_blocks_per_sm
         t.leaf_threads = leaf_threads

@@ -361,6 +361,114 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     if ((threadIdx.x & 31) == 0 && counted) atomicAdd(counter + 1, (unsigned long long)counted);
 }
 
+// Persistent table leaf that keeps every warp counting (pb_tuning.tt_leaf =
+// 2).  In k_leaf2_tt a thread whose edge hits the table idles through its
+// CTA's grandchild loop, and a CTA holds its registers until its last warp
+// is done, so at the leaf's ~45 % hit rate nearly half the warps of the SM
+// have nothing to do.  Here each CTA takes T edges at a time from an atomic
+// cursor, makes their children, probes the depth-2 table (hits are written
+// at once) and appends each miss (edge index, key) to a shared-memory queue;
+// whenever the queue holds T misses, or the edges are exhausted, the CTA
+// takes T of them, remakes their children from the parent and the move,
+// ranks them by move count and counts their grandchildren.  The queue holds
+// at most 2T entries: the count passes drain it while it holds T, and one
+// probe round adds at most T.  MODE is the leaf mode (1 or 2).
+template <int C, bool STRICT, int MODE>
+__global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
+    k_leaf2_tt_fill(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                    const Hash128 *__restrict__ phash, const u32 *__restrict__ pidx,
+                    const uint16_t *__restrict__ moves, u64 n, u64 nparents, TTView tt, u32 *__restrict__ out,
+                    unsigned long long *__restrict__ cursor, unsigned long long *__restrict__ counter)
+{
+    constexpr int T = PB_LEAF_THREADS;
+    constexpr int Q = 2 * T;
+    __shared__ u32 q_i[Q];
+    __shared__ Hash128 q_h[Q];
+    __shared__ u32 q_n;
+    __shared__ unsigned long long s_base;
+    __shared__ Board s_b[T];
+    __shared__ Hash128 s_h[T];
+    __shared__ u32 s_i[T];
+    __shared__ uint8_t s_st[T];
+    __shared__ uint8_t s_key[T];
+    const int tid = threadIdx.x;
+    u32 counted = 0;
+    if (tid == 0) q_n = 0;
+    for (;;) {
+        if (tid == 0) s_base = atomicAdd(cursor, (unsigned long long)T);
+        __syncthreads();
+        const u64 base = s_base;
+        const bool done = base >= n;
+        if (!done) {
+            const u64 i = base + tid;
+            if (i < n && pidx[i] < nparents) {
+                const u32 p = pidx[i];
+                Board b = load_board(pboards + p);
+                u32 st = pstates[p];
+                const Board before = b;
+                const uint16_t mv0 = moves[i];
+                make_move<C>(b, st, mv0);
+                const Hash128 h = hash_move(phash[p], before, pstates[p], st, C, mv0);
+                u64 hit;
+                if (tt_probe(tt, h, &hit)) {
+                    out[i] = (u32)hit;
+                } else {
+                    const u32 slot = atomicAdd(&q_n, 1u);
+                    q_i[slot] = (u32)i;
+                    q_h[slot] = h;
+                }
+            }
+        }
+        __syncthreads();
+        // count passes over full CTAs of misses (the rest once the edges are done)
+        for (;;) {
+            const u32 qn = q_n;
+            if (!(qn >= (u32)T || (done && qn > 0))) break;
+            const u32 take = min(qn, (u32)T), first = qn - take;
+            bool miss = (u32)tid < take;
+            Board b{};
+            u32 st = 0, i = 0;
+            Hash128 h{};
+            if (miss) {
+                i = q_i[first + tid];
+                h = q_h[first + tid];
+                const u32 p = pidx[i];
+                b = load_board(pboards + p);
+                st = pstates[p];
+                make_move<C>(b, st, moves[i]);
+            }
+            __syncthreads();  // every entry read before the queue shrinks
+            if (tid == 0) q_n = first;
+            const u32 key = miss ? 1 + min(count_moves<1 - C, true>(b, st), 254u) : 0u;
+            const u32 rank = cta_rank_u8<T>(key);
+            s_b[rank] = b;
+            s_h[rank] = h;
+            s_i[rank] = i;
+            s_st[rank] = (uint8_t)st;
+            s_key[rank] = (uint8_t)key;
+            __syncthreads();
+            b = s_b[tid];
+            h = s_h[tid];
+            i = s_i[tid];
+            st = s_st[tid];
+            miss = s_key[tid] != 0;
+            if (miss) {
+                uint16_t mv[MAX_MOVES];
+                ArraySink sink{mv, 0};
+                gen_moves<1 - C>(b, st, sink);
+                const u32 total = grandchild_counts<C, STRICT, MODE == 2, T>(b, st, mv, sink.n);
+                counted += sink.n;
+                tt_store(tt, h, total);
+                out[i] = total;
+            }
+            __syncthreads();  // exchange arrays and q_n settled before the next pass
+        }
+        if (done) break;
+    }
+    counted = __reduce_add_sync(0xffffffffu, counted);
+    if ((tid & 31) == 0 && counted) atomicAdd(counter + 1, (unsigned long long)counted);
+}
+
 // Upsweep of one level: vals[i] = sum of the children's counts over
 // [offs[i], offs[i] + counts[i]) unless i was a TT hit or a duplicate; the
 // result is stored in TT[r].

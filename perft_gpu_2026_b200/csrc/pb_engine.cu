@@ -73,7 +73,7 @@ struct pb_ctx {
     u64 *h_pinned = nullptr;  // pinned host words for readbacks
     int launch_depth = 0;
     bool timing = false;
-    pb_tuning tuning{5, 0, 256, 128, 2, 1, 1, 1};
+    pb_tuning tuning{5, 0, 256, 128, 2, 1, 1, 1, 1};
     int num_sms = 0;
     uint16_t *spill = nullptr;  // cooperative-leaf spill area (device)
     size_t spill_blocks = 0;
@@ -432,6 +432,42 @@ struct TTLevel {
     int rem;
 };
 
+// The persistent table leaf: one CTA per resident slot, at most one per T edges.
+template <int C, bool S, int MODE>
+int launch_tt_fill_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const Hash128 *h, const u32 *pi,
+                     const uint16_t *mv, u64 n, u64 npar, TTView tv, u32 *out, unsigned long long *cursor)
+{
+    int per_sm = 0;
+    PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_leaf2_tt_fill<C, S, MODE>, PB_LEAF_THREADS, 0));
+    if (per_sm <= 0) per_sm = 1;
+    const u64 grid = std::min<u64>((u64)ctx->num_sms * per_sm, (n + PB_LEAF_THREADS - 1) / PB_LEAF_THREADS);
+    k_leaf2_tt_fill<C, S, MODE><<<(unsigned)grid, PB_LEAF_THREADS, 0, ctx->stream>>>(b, st, h, pi, mv, n, npar, tv, out,
+                                                                                     cursor, ctx->d_counter);
+    PB_CUDA(cudaGetLastError());
+    return PB_OK;
+}
+int launch_tt_fill(pb_ctx *ctx, int c, bool strict, int mode, const Board *b, const uint8_t *st, const Hash128 *h,
+                   const u32 *pi, const uint16_t *mv, u64 n, u64 npar, TTView tv, u32 *out,
+                   unsigned long long *cursor)
+{
+#define PB_FILL(CC, SS, MM) return launch_tt_fill_t<CC, SS, MM>(ctx, b, st, h, pi, mv, n, npar, tv, out, cursor)
+    if (c == WHITE) {
+        if (strict) {
+            if (mode == 2) PB_FILL(WHITE, true, 2);
+            PB_FILL(WHITE, true, 1);
+        }
+        if (mode == 2) PB_FILL(WHITE, false, 2);
+        PB_FILL(WHITE, false, 1);
+    }
+    if (strict) {
+        if (mode == 2) PB_FILL(BLACK, true, 2);
+        PB_FILL(BLACK, true, 1);
+    }
+    if (mode == 2) PB_FILL(BLACK, false, 2);
+    PB_FILL(BLACK, false, 1);
+#undef PB_FILL
+}
+
 // GPU breadth-first perft with the device TTs (perft_gpu_host_bfs with
 // g_useTT, perft_kernels.cu:620-990) of n roots of one colour at once: probe
 // at every level, dedup (across all the roots' subtrees of a level), leaf TT,
@@ -624,13 +660,20 @@ int bfs_tt_roots(pb_ctx *ctx, const Board *rb, const uint8_t *rs, const Hash128 
     }
     // leaf: per-edge perft(2) with the depth-2 table
     u32 *leafcnt = ar.take<u32>(n > 0 ? n : 1);
-    if (!leafcnt) {
+    unsigned long long *cursor = ar.take<unsigned long long>(1);
+    if (!leafcnt || !cursor) {
         *bfs_status = BFS_TOO_BIG;
         return PB_OK;
     }
     PB_CUDA(cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(unsigned long long), s));
     if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[1], s));
-    if (n > 0) {
+    if (n > 0 && leaf_mode(ctx) >= 1 && ctx->tuning.tt_leaf == 2) {
+        PB_CUDA(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s));
+        int rc2 = launch_tt_fill(ctx, c, strict, leaf_mode(ctx), cur_b, cur_s, cur_h, epi, emv, n, n_par,
+                                 ctx->dtt.at(2), leafcnt, cursor);
+        if (rc2 != PB_OK) return rc2;
+        stats.kernels += 1;
+    } else if (n > 0) {
         TTView tv = ctx->dtt.at(2);
         unsigned g = grid_for(n, PB_LEAF_THREADS);
         const int mode = leaf_mode(ctx);
@@ -1954,6 +1997,10 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
     if (t->host_driver) {
         if (t->host_driver != 1 && t->host_driver != 2) return PB_ERR_ARG;
         ctx->tuning.host_driver = t->host_driver;
+    }
+    if (t->tt_leaf) {
+        if (t->tt_leaf != 1 && t->tt_leaf != 2) return PB_ERR_ARG;
+        ctx->tuning.tt_leaf = t->tt_leaf;
     }
     return PB_OK;
 }

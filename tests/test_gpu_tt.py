@@ -130,3 +130,25 @@ def test_table_leaf_modes_match_fixtures(golden, leaf_kernel):
     assert not bad, bad
     assert eng.perft_position(pg.config_position(4, 1), 7) == 26402736244
     eng.close()
+
+
+@pytest.mark.parametrize("leaf_kernel", [4, 5])
+def test_persistent_table_leaf_stays_exact(golden, leaf_kernel):
+    """tt_leaf 2: CTAs queue their table misses in shared memory and count
+    only full CTAs of misses.  Against the fixtures, the bench position at
+    perft 7 and the README totals, with tables large (many hits) and tiny
+    (nearly all misses, constant overwrites)."""
+    for dtt in (2048, 1):
+        eng = pg.Engine(device=0, use_tt=True, arena_bytes=2 << 30, device_tt_mb=dtt, host_tt_mb=256)
+        eng.set_tuning(leaf_kernel=leaf_kernel, tt_leaf=2)
+        bad = []
+        for case in golden:
+            p = pg.parse_fen(case["fen"])
+            for d, want in enumerate(case["counts"], start=1):
+                got = eng.perft_position(p, d)
+                if got != want:
+                    bad.append((case["name"], d, got, want))
+        assert not bad, (dtt, bad)
+        assert eng.perft_position(pg.config_position(4, 1), 7) == 26402736244
+        assert eng.perft_position(pg.parse_fen(START), 8) == 84998978956
+        eng.close()
