@@ -199,9 +199,9 @@ typedef struct {
                            call per subtree (perft_cpu_recurse, launcher.cu:572-715; default);
                            2 = breadth first, transpositions merged by key with tables, the
                            launch-depth positions in batched GPU calls */
-    int tt_leaf;        /* table leaf with leaf kernels 4 and 5: 1 = one edge per thread (default);
+    int tt_leaf;        /* table leaf with leaf kernels 4 and 5: 1 = one edge per thread;
                            2 = persistent CTAs that queue their table misses in shared memory and
-                           count only full CTAs of misses */
+                           count only full CTAs of misses (default) */
 } pb_tuning;
 
 int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t);

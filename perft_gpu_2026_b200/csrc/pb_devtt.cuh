@@ -372,7 +372,11 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
 // takes T of them, remakes their children from the parent and the move,
 // ranks them by move count and counts their grandchildren.  The queue holds
 // at most 2T entries: the count passes drain it while it holds T, and one
-// probe round adds at most T.  MODE is the leaf mode (1 or 2).
+// probe round adds at most T.  MODE is the leaf mode (1 or 2).  Measured on
+// B200 against k_leaf2_tt (same counts): start position perft 10 with 150 GB
+// of tables 1.923 -> 1.787 s, the 2-ply seed-4 position perft 10 3.487 ->
+// 3.240 s (27.4 -> 30.1 G move-count calls/s), start position perft 9 with
+// 16 GB 171.8 -> 163.6 ms of leaf time.
 template <int C, bool STRICT, int MODE>
 __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     k_leaf2_tt_fill(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
