@@ -99,7 +99,8 @@ def cpu_model() -> str:
 
 
 # leaf kernel launched for each pb_tuning.leaf_kernel value
-LEAF_KERNELS = {1: "k_leaf2", 2: "k_leaf2_coop", 3: "k_leaf2_defer", 4: "k_leaf2_sorted", 5: "k_leaf2_listed"}
+LEAF_KERNELS = {1: "k_leaf2", 2: "k_leaf2_coop", 3: "k_leaf2_defer", 4: "k_leaf2_sorted", 5: "k_leaf2_listed",
+                6: "k_leaf2_balanced"}
 
 
 def _load_profile_constants():

@@ -2,7 +2,8 @@
 
 Candidates: leaf kernel (one edge per thread / cooperative / one edge per
 thread with the CTA's children ranked by move count / ranked with each
-child's own-piece squares listed once), the leaf's CTA size
+child's own-piece squares listed once / the same with four children per
+thread balanced across the warps), the leaf's CTA size
 (128/256/512), the staged generator's CTA size and tile (64 or 128
 threads, 64 moves staged per thread) and the leaf fuse depth (two plies fused
 in the leaf, or one with an extra BFS level).  Each candidate runs perft 7
@@ -43,7 +44,7 @@ def candidates() -> List[Dict[str, int]]:
     for lt, gt, fuse in itertools.product((128, 256, 512), (64, 128), (2, 1)):
         out.append({"leaf_kernel": 1, "leaf_threads": lt, "gen_threads": gt, "leaf_fuse": fuse})
     out.append({"leaf_kernel": 2, "leaf_threads": 256, "gen_threads": 128, "leaf_fuse": 2})
-    for lk in (4, 5):
+    for lk in (4, 5, 6):
         for gt in (64, 128):
             out.append({"leaf_kernel": lk, "leaf_threads": 256, "gen_threads": gt, "leaf_fuse": 2})
     return out

@@ -180,10 +180,10 @@ struct Arena {
 inline unsigned grid_for(u64 n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 // Leaf mode of the batched, planned and table leaves (grandchild_counts):
-// 2 for leaf kernel 5 (ranked, listed pieces), 1 for 4 (ranked), else 0.
+// 2 for leaf kernels 5 and 6 (ranked, listed pieces), 1 for 4 (ranked), else 0.
 inline int leaf_mode(const pb_ctx *ctx)
 {
-    return ctx->tuning.leaf_kernel == 5 ? 2 : ctx->tuning.leaf_kernel == 4 ? 1 : 0;
+    return ctx->tuning.leaf_kernel >= 5 ? 2 : ctx->tuning.leaf_kernel == 4 ? 1 : 0;
 }
 
 // NVTX range for profilers (header-only NVTX v3: free unless a tool attaches):
@@ -211,6 +211,18 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
         switch (ctx->tuning.leaf_threads) {
         case 128: k_leaf2_defer<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         default: k_leaf2_defer<C, S, 256><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        }
+        PB_CUDA(cudaGetLastError());
+        return PB_OK;
+    }
+    if (ctx->tuning.leaf_kernel == 6) {
+        // four edges per thread
+        const u64 per = 4ull * (u64)ctx->tuning.leaf_threads;
+        const unsigned g = (unsigned)((n + per - 1) / per);
+        switch (ctx->tuning.leaf_threads) {
+        case 128: k_leaf2_balanced<C, S, 128><<<g, 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        case 512: k_leaf2_balanced<C, S, 512><<<g, 512, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        default: k_leaf2_balanced<C, S, 256><<<g, 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         }
         PB_CUDA(cudaGetLastError());
         return PB_OK;
@@ -1963,7 +1975,7 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
 {
     if (!ctx || !t) return PB_ERR_ARG;
     if (t->leaf_kernel) {
-        if (t->leaf_kernel < 1 || t->leaf_kernel > 5) return PB_ERR_ARG;
+        if (t->leaf_kernel < 1 || t->leaf_kernel > 6) return PB_ERR_ARG;
         ctx->tuning.leaf_kernel = t->leaf_kernel;
     }
     if (t->leaf_blocks_per_sm) {

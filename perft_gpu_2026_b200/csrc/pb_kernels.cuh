@@ -593,6 +593,75 @@ __global__ void __launch_bounds__(T, PB_LISTED_WARPS_PER_SM * 32 / T) k_leaf2_li
     }
 }
 
+// Ranked leaf with work balanced across the CTA's warps (leaf kernel 6).  In
+// the ranked leaves warp 0 gets the CTA's lightest children and the last warp
+// the heaviest; a warp that finishes early keeps its registers until its
+// CTA ends, so on the bench position only 26.6 of the 32 resident warps were
+// active on average.  Here each thread makes K = 4 children (the CTA covers
+// 4T edges) and counts their moves; the 4T children are ranked by move count
+// and cut into 32-child chunks in rank order; chunk j is paired with chunk
+// NCH - 1 - j (a light and a heavy one) and pair j goes to warp j % W, so
+// every warp gets about the same work while the lanes of a chunk still have
+// similar loop lengths.  Only edge indices pass through shared memory (4 B
+// per child): each lane remakes its child from the parent and the move, then
+// generates its moves and counts the grandchildren with listed pieces.
+template <int C, bool STRICT, int T>
+__global__ void __launch_bounds__(T, 1024 / T) k_leaf2_balanced(const Board *__restrict__ pboards,
+                                                                const uint8_t *__restrict__ pstates,
+                                                                const u32 *__restrict__ pidx,
+                                                                const uint16_t *__restrict__ moves, u64 n,
+                                                                u64 nparents, unsigned long long *__restrict__ counter)
+{
+    constexpr int K = 4;
+    constexpr int W = T / 32;
+    constexpr int NCH = K * T / 32;
+    static_assert(NCH == 2 * 2 * W, "two chunk pairs per warp");
+    constexpr u32 NONE = 0xFFFFFFFFu;
+    __shared__ u32 s_edge[K * T];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u64 first = (u64)blockIdx.x * (K * T);
+    u32 key[K], rank[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const u64 i = first + (u64)k * T + tid;
+        key[k] = 0;
+        if (i < n && pidx[i] < nparents) {
+            const u32 p = pidx[i];
+            Board b = load_board(pboards + p);
+            u32 st = pstates[p];
+            make_move<C>(b, st, moves[i]);
+            key[k] = 1 + min(count_moves<1 - C, true>(b, st), 254u);
+        }
+    }
+    cta_rank_u8<T, K>(key, rank);
+#pragma unroll
+    for (int k = 0; k < K; k++) s_edge[rank[k]] = key[k] ? (u32)(first + (u64)k * T + tid) : NONE;
+    __syncthreads();
+    u32 total = 0, counted = 0;
+    for (int q = 0; q < K; q++) {
+        const int pair = warp + (q >> 1) * W;
+        const int chunk = (q & 1) ? NCH - 1 - pair : pair;
+        const u32 e = s_edge[chunk * 32 + lane];
+        if (e != NONE) {
+            const u32 p = pidx[e];
+            Board b = load_board(pboards + p);
+            u32 st = pstates[p];
+            make_move<C>(b, st, moves[e]);
+            uint16_t mv[MAX_MOVES];
+            ArraySink sink{mv, 0};
+            gen_moves<1 - C>(b, st, sink);
+            total += grandchild_counts<C, STRICT, true, T>(b, st, mv, sink.n);
+            counted += sink.n;
+        }
+    }
+    total = __reduce_add_sync(0xffffffffu, total);
+    counted = __reduce_add_sync(0xffffffffu, counted);
+    if (lane == 0 && counted) {
+        atomicAdd(counter, (unsigned long long)total);
+        atomicAdd(counter + 1, (unsigned long long)counted);
+    }
+}
+
 // ---------------------------------------------------------------- cooperative leaf
 // Fused two-ply leaf with the grandchild work spread over the whole CTA.
 //

@@ -49,7 +49,7 @@ def test_scan_unaligned_and_many_tiles(gpu_engine):
         assert int(d_tot.item()) == int(x.sum()), (n, shift)
 
 
-@pytest.mark.parametrize("leaf_kernel", [1, 2, 4, 5])
+@pytest.mark.parametrize("leaf_kernel", [1, 2, 4, 5, 6])
 def test_gpu_matches_reference_fixtures(gpu_engine, golden, leaf_kernel):
     prev = gpu_engine.get_tuning().leaf_kernel
     gpu_engine.set_tuning(leaf_kernel=leaf_kernel)
@@ -89,7 +89,7 @@ def test_strict_mode_counts_merged_moves(oracle):
     comp.close()
 
 
-@pytest.mark.parametrize("leaf_kernel", [1, 2, 4, 5])
+@pytest.mark.parametrize("leaf_kernel", [1, 2, 4, 5, 6])
 def test_readme_known_totals(gpu_engine, leaf_kernel):
     # README.md:51-52 and :92 (RTX PRO 6000 / GB10 tables)
     prev = gpu_engine.get_tuning().leaf_kernel
@@ -270,14 +270,15 @@ def test_batched_leaf_ranked_and_unranked_agree():
     eng.close()
 
 
+@pytest.mark.parametrize("leaf_kernel", [5, 6])
 @pytest.mark.parametrize("threads", [128, 256, 512])
-def test_listed_piece_leaf_on_playouts(threads, oracle):
+def test_listed_piece_leaf_on_playouts(threads, leaf_kernel, oracle):
     """Leaf kernel 5 (own-piece squares listed once per child) against the
     oracle on playout positions of every game phase, both colours to move,
     including positions with promoted pieces (more than four of a kind fall
     back to the bitboard count)."""
     eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
-    eng.set_tuning(leaf_kernel=5, leaf_threads=threads)
+    eng.set_tuning(leaf_kernel=leaf_kernel, leaf_threads=threads)
     roots = [p for p in pg.random_playouts(4747, 40, 0, 160) if pg.count_moves(p, True) > 0]
     for p in roots:
         fen = pg.to_fen(p)
