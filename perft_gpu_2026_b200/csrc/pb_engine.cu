@@ -216,12 +216,13 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
         return PB_OK;
     }
     if (ctx->tuning.leaf_kernel == 6) {
-        // four edges per thread
-        const u64 per = 4ull * (u64)ctx->tuning.leaf_threads;
+        // PB_BALANCED_K edges per thread
+        const u64 per = (u64)PB_BALANCED_K * (u64)ctx->tuning.leaf_threads;
         const unsigned g = (unsigned)((n + per - 1) / per);
         switch (ctx->tuning.leaf_threads) {
         case 128: k_leaf2_balanced<C, S, 128><<<g, 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         case 512: k_leaf2_balanced<C, S, 512><<<g, 512, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
+        case 1024: k_leaf2_balanced<C, S, 1024><<<g, 1024, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         default: k_leaf2_balanced<C, S, 256><<<g, 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         }
         PB_CUDA(cudaGetLastError());
@@ -1983,7 +1984,10 @@ int pb_set_tuning(pb_ctx *ctx, const pb_tuning *t)
         ctx->tuning.leaf_blocks_per_sm = t->leaf_blocks_per_sm;
     }
     if (t->leaf_threads) {
-        if (t->leaf_threads != 128 && t->leaf_threads != 256 && t->leaf_threads != 512) return PB_ERR_ARG;
+        const int lk = t->leaf_kernel ? t->leaf_kernel : ctx->tuning.leaf_kernel;
+        if (t->leaf_threads != 128 && t->leaf_threads != 256 && t->leaf_threads != 512 &&
+            !(t->leaf_threads == 1024 && lk == 6))
+            return PB_ERR_ARG;
         ctx->tuning.leaf_threads = t->leaf_threads;
     }
     if (t->gen_threads) {

@@ -597,14 +597,17 @@ __global__ void __launch_bounds__(T, PB_LISTED_WARPS_PER_SM * 32 / T) k_leaf2_li
 // the ranked leaves warp 0 gets the CTA's lightest children and the last warp
 // the heaviest; a warp that finishes early keeps its registers until its
 // CTA ends, so on the bench position only 26.6 of the 32 resident warps were
-// active on average.  Here each thread makes K = 4 children (the CTA covers
-// 4T edges) and counts their moves; the 4T children are ranked by move count
+// active on average.  Here each thread makes K = PB_BALANCED_K children (the
+// CTA covers KT edges) and counts their moves; the 4T children are ranked by move count
 // and cut into 32-child chunks in rank order; chunk j is paired with chunk
 // NCH - 1 - j (a light and a heavy one) and pair j goes to warp j % W, so
 // every warp gets about the same work while the lanes of a chunk still have
 // similar loop lengths.  Only edge indices pass through shared memory (4 B
 // per child): each lane remakes its child from the parent and the move, then
 // generates its moves and counts the grandchildren with listed pieces.
+#ifndef PB_BALANCED_K
+#define PB_BALANCED_K 4  // children per thread of k_leaf2_balanced
+#endif
 template <int C, bool STRICT, int T>
 __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_balanced(const Board *__restrict__ pboards,
                                                                 const uint8_t *__restrict__ pstates,
@@ -612,10 +615,10 @@ __global__ void __launch_bounds__(T, 1024 / T) k_leaf2_balanced(const Board *__r
                                                                 const uint16_t *__restrict__ moves, u64 n,
                                                                 u64 nparents, unsigned long long *__restrict__ counter)
 {
-    constexpr int K = 4;
+    constexpr int K = PB_BALANCED_K;
     constexpr int W = T / 32;
     constexpr int NCH = K * T / 32;
-    static_assert(NCH == 2 * 2 * W, "two chunk pairs per warp");
+    static_assert(K % 2 == 0 && NCH == K * W, "K/2 chunk pairs per warp");
     constexpr u32 NONE = 0xFFFFFFFFu;
     __shared__ u32 s_edge[K * T];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

@@ -270,8 +270,8 @@ def test_batched_leaf_ranked_and_unranked_agree():
     eng.close()
 
 
-@pytest.mark.parametrize("leaf_kernel", [5, 6])
-@pytest.mark.parametrize("threads", [128, 256, 512])
+@pytest.mark.parametrize("leaf_kernel,threads", [(5, 128), (5, 256), (5, 512), (6, 128), (6, 256), (6, 512),
+                                                  (6, 1024)])
 def test_listed_piece_leaf_on_playouts(threads, leaf_kernel, oracle):
     """Leaf kernel 5 (own-piece squares listed once per child) against the
     oracle on playout positions of every game phase, both colours to move,
