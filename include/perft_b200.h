@@ -180,15 +180,16 @@ typedef struct {
  * 2 = cooperative (grandchildren spread over the CTA), 3 = in-check children
  * deferred to a second pass, 4 = one edge per thread with the CTA's children
  * ranked by move count first, 5 = as 4 with each child's own-piece squares
- * listed once for all of its grandchild counts (default), 6 = as 5 with four
- * children per thread ranked across the CTA and dealt to the warps in
- * light/heavy chunk pairs (batched, planned and table leaves rank their
- * children for 4 to 6 and list pieces for 5 and 6);
+ * listed once for all of its grandchild counts, 6 = as 5 with four children
+ * per thread ranked across the CTA and dealt to the warps in light/heavy
+ * chunk pairs (default, with 1024-thread CTAs); batched, planned and table
+ * leaves rank their children for 4 to 6 and list pieces for 5 and 6;
  * leaf_blocks_per_sm: persistent grid of the cooperative leaf. */
 typedef struct {
     int leaf_kernel;
     int leaf_blocks_per_sm;
-    int leaf_threads;   /* CTA size of leaf kernels 1, 3 to 6: 128, 256 (default) or 512 (not 3) */
+    int leaf_threads;   /* CTA size of leaf kernels 1, 3 to 6: 128, 256, 512 (not 3) or, with leaf
+                           kernel 6 only, 1024 (default; other kernels then run 256) */
     int gen_threads;    /* CTA size of the staged generator: 64 or 128 (default); stages 64 moves per thread */
     int leaf_fuse;      /* plies fused in the leaf kernel: 2 (default) or 1 (one more BFS level) */
     int tt_replace;     /* device TT replacement: 1 = always overwrite (default, tt.h:60-70),

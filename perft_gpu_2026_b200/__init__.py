@@ -434,9 +434,10 @@ class Engine:
         """Launch parameters (pb_set_tuning); 0 keeps the current value.
         leaf_kernel 1 = one edge per thread, 2 = cooperative, 3 = in-check
         children deferred, 4 = children ranked by move count,
-        5 = ranked with each child's own-piece squares listed once (default),
-        6 = as 5 with four children per thread balanced across the warps;
-        leaf_threads 128/256/512; gen_threads 64/128; leaf_fuse 1/2;
+        5 = ranked with each child's own-piece squares listed once,
+        6 = as 5 with four children per thread balanced across the warps
+        (default); leaf_threads 128/256/512, or 1024 with leaf kernel 6
+        (default); gen_threads 64/128; leaf_fuse 1/2;
         tt_replace 1 = always overwrite, 2 = two-slot size priority;
         planned_leaf 1 = grid over the planned capacity (default),
         2 = persistent work-queue leaf; host_driver 1 = depth-first tree

@@ -44,9 +44,12 @@ def candidates() -> List[Dict[str, int]]:
     for lt, gt, fuse in itertools.product((128, 256, 512), (64, 128), (2, 1)):
         out.append({"leaf_kernel": 1, "leaf_threads": lt, "gen_threads": gt, "leaf_fuse": fuse})
     out.append({"leaf_kernel": 2, "leaf_threads": 256, "gen_threads": 128, "leaf_fuse": 2})
-    for lk in (4, 5, 6):
+    for lk in (4, 5):
         for gt in (64, 128):
             out.append({"leaf_kernel": lk, "leaf_threads": 256, "gen_threads": gt, "leaf_fuse": 2})
+    for lt in (512, 1024):
+        for gt in (64, 128):
+            out.append({"leaf_kernel": 6, "leaf_threads": lt, "gen_threads": gt, "leaf_fuse": 2})
     return out
 
 

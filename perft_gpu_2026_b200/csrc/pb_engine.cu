@@ -73,7 +73,7 @@ struct pb_ctx {
     u64 *h_pinned = nullptr;  // pinned host words for readbacks
     int launch_depth = 0;
     bool timing = false;
-    pb_tuning tuning{5, 0, 256, 128, 2, 1, 1, 1, 2};
+    pb_tuning tuning{6, 0, 1024, 128, 2, 1, 1, 1, 2};
     int num_sms = 0;
     uint16_t *spill = nullptr;  // cooperative-leaf spill area (device)
     size_t spill_blocks = 0;
