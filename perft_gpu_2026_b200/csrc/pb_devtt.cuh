@@ -368,11 +368,14 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
 // have nothing to do.  Here each CTA takes T edges at a time from an atomic
 // cursor, makes their children, probes the depth-2 table (hits are written
 // at once) and appends each miss (edge index, key) to a shared-memory queue;
-// whenever the queue holds T misses, or the edges are exhausted, the CTA
-// takes T of them, remakes their children from the parent and the move,
-// ranks them by move count and counts their grandchildren.  The queue holds
-// at most 2T entries: the count passes drain it while it holds T, and one
-// probe round adds at most T.  MODE is the leaf mode (1 or 2).  Measured on
+// whenever the queue holds 2T misses, or the edges are exhausted, the CTA
+// takes 2T of them (two per thread), remakes their children from the parent
+// and the move, ranks them by move count and cuts the ranking into 32-miss
+// chunks; warp w counts chunks w and 2W - 1 - w (a light and a heavy one),
+// so the warps of a pass reach its closing barrier at about the same time
+// while the lanes of a chunk still have similar loop lengths.  The queue
+// holds at most 3T entries: the passes drain it below 2T, and one probe round
+// adds at most T.  MODE is the leaf mode (1 or 2).  Measured on
 // B200 against k_leaf2_tt (same counts): start position perft 10 with 150 GB
 // of tables 1.923 -> 1.787 s, the 2-ply seed-4 position perft 10 3.487 ->
 // 3.240 s (27.4 -> 30.1 G move-count calls/s), start position perft 9 with
@@ -385,17 +388,18 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
                     unsigned long long *__restrict__ cursor, unsigned long long *__restrict__ counter)
 {
     constexpr int T = PB_LEAF_THREADS;
-    constexpr int Q = 2 * T;
+    constexpr int PASS = 2 * T;      // misses per count pass, two per thread
+    constexpr int Q = PASS + T;      // drained below PASS; one probe round adds at most T
+    constexpr int W = T / 32;
+    constexpr int NCH = PASS / 32;   // 32-miss chunks of a pass, paired (j, NCH - 1 - j) per warp
+    static_assert(NCH == 2 * W, "one chunk pair per warp");
+    constexpr u32 NONE = 0xFFFFFFFFu;
     __shared__ u32 q_i[Q];
     __shared__ Hash128 q_h[Q];
+    __shared__ u32 s_slot[PASS];
     __shared__ u32 q_n;
     __shared__ unsigned long long s_base;
-    __shared__ Board s_b[T];
-    __shared__ Hash128 s_h[T];
-    __shared__ u32 s_i[T];
-    __shared__ uint8_t s_st[T];
-    __shared__ uint8_t s_key[T];
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     u32 counted = 0;
     if (tid == 0) q_n = 0;
     for (;;) {
@@ -424,48 +428,50 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
             }
         }
         __syncthreads();
-        // count passes over full CTAs of misses (the rest once the edges are done)
+        // count passes over PASS misses (the rest once the edges are done)
         for (;;) {
             const u32 qn = q_n;
-            if (!(qn >= (u32)T || (done && qn > 0))) break;
-            const u32 take = min(qn, (u32)T), first = qn - take;
-            bool miss = (u32)tid < take;
-            Board b{};
-            u32 st = 0, i = 0;
-            Hash128 h{};
-            if (miss) {
-                i = q_i[first + tid];
-                h = q_h[first + tid];
-                const u32 p = pidx[i];
-                b = load_board(pboards + p);
-                st = pstates[p];
-                make_move<C>(b, st, moves[i]);
+            if (!(qn >= (u32)PASS || (done && qn > 0))) break;
+            const u32 take = min(qn, (u32)PASS), first = qn - take;
+            u32 key[2], rank[2];
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const u32 e = (u32)(k * T + tid);
+                key[k] = 0;
+                if (e < take) {
+                    const u32 i = q_i[first + e], p = pidx[i];
+                    Board b = load_board(pboards + p);
+                    u32 st = pstates[p];
+                    make_move<C>(b, st, moves[i]);
+                    key[k] = 1 + min(count_moves<1 - C, true>(b, st), 254u);
+                }
             }
-            __syncthreads();  // every entry read before the queue shrinks
-            if (tid == 0) q_n = first;
-            const u32 key = miss ? 1 + min(count_moves<1 - C, true>(b, st), 254u) : 0u;
-            const u32 rank = cta_rank_u8<T>(key);
-            s_b[rank] = b;
-            s_h[rank] = h;
-            s_i[rank] = i;
-            s_st[rank] = (uint8_t)st;
-            s_key[rank] = (uint8_t)key;
+            cta_rank_u8<T, 2>(key, rank);
+#pragma unroll
+            for (int k = 0; k < 2; k++) s_slot[rank[k]] = key[k] ? first + (u32)(k * T + tid) : NONE;
             __syncthreads();
-            b = s_b[tid];
-            h = s_h[tid];
-            i = s_i[tid];
-            st = s_st[tid];
-            miss = s_key[tid] != 0;
-            if (miss) {
-                uint16_t mv[MAX_MOVES];
-                ArraySink sink{mv, 0};
-                gen_moves<1 - C>(b, st, sink);
-                const u32 total = grandchild_counts<C, STRICT, MODE == 2, T>(b, st, mv, sink.n);
-                counted += sink.n;
-                tt_store(tt, h, total);
-                out[i] = total;
+#pragma unroll 1
+            for (int q = 0; q < 2; q++) {
+                const int chunk = q ? NCH - 1 - warp : warp;
+                const u32 slot = s_slot[chunk * 32 + lane];
+                if (slot != NONE) {
+                    const u32 i = q_i[slot], p = pidx[i];
+                    const Hash128 h = q_h[slot];
+                    Board b = load_board(pboards + p);
+                    u32 st = pstates[p];
+                    make_move<C>(b, st, moves[i]);
+                    uint16_t mv[MAX_MOVES];
+                    ArraySink sink{mv, 0};
+                    gen_moves<1 - C>(b, st, sink);
+                    const u32 total = grandchild_counts<C, STRICT, MODE == 2, T>(b, st, mv, sink.n);
+                    counted += sink.n;
+                    tt_store(tt, h, total);
+                    out[i] = total;
+                }
             }
-            __syncthreads();  // exchange arrays and q_n settled before the next pass
+            __syncthreads();  // every queued entry of the pass read
+            if (tid == 0) q_n = first;
+            __syncthreads();
         }
         if (done) break;
     }
