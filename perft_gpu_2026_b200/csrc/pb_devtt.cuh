@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
         uint16_t mv[MAX_MOVES];
         ArraySink sink{mv, 0};
         gen_moves<1 - C>(b, st, sink);
-        total = grandchild_counts<C, STRICT, MODE == 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
+        total = grandchild_counts<C, STRICT, MODE >= 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
         counted = sink.n;
         tt_store(tt, h, total);
         out[i] = total;
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
                     uint16_t mv[MAX_MOVES];
                     ArraySink sink{mv, 0};
                     gen_moves<1 - C>(b, st, sink);
-                    const u32 total = grandchild_counts<C, STRICT, MODE == 2, T>(b, st, mv, sink.n);
+                    const u32 total = grandchild_counts<C, STRICT, MODE >= 2, T>(b, st, mv, sink.n);
                     counted += sink.n;
                     tt_store(tt, h, total);
                     out[i] = total;

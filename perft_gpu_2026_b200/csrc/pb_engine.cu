@@ -180,10 +180,21 @@ struct Arena {
 inline unsigned grid_for(u64 n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 // Leaf mode of the batched, planned and table leaves (grandchild_counts):
-// 2 for leaf kernels 5 and 6 (ranked, listed pieces), 1 for 4 (ranked), else 0.
+// 3 for leaf kernel 6 (ranked, listed pieces, balanced warps), 2 for 5
+// (ranked, listed pieces), 1 for 4 (ranked), else 0.
 inline int leaf_mode(const pb_ctx *ctx)
 {
-    return ctx->tuning.leaf_kernel >= 5 ? 2 : ctx->tuning.leaf_kernel == 4 ? 1 : 0;
+    return ctx->tuning.leaf_kernel == 6 ? 3 : ctx->tuning.leaf_kernel == 5 ? 2 : ctx->tuning.leaf_kernel == 4 ? 1 : 0;
+}
+
+// CTA size of a balanced leaf over n edges (PB_BALANCED_K per thread): the
+// tuned size, halved down to 256 while the grid would have fewer than 8 CTAs
+// per SM (a small launch of big CTAs leaves its last wave half empty).
+inline int balanced_threads(const pb_ctx *ctx, u64 n, int tuned)
+{
+    int t = tuned;
+    while (t > 256 && n < (u64)PB_BALANCED_K * (u64)t * 8u * (u64)ctx->num_sms) t /= 2;
+    return t;
 }
 
 // NVTX range for profilers (header-only NVTX v3: free unless a tool attaches):
@@ -217,9 +228,10 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
     }
     if (ctx->tuning.leaf_kernel == 6) {
         // PB_BALANCED_K edges per thread
-        const u64 per = (u64)PB_BALANCED_K * (u64)ctx->tuning.leaf_threads;
+        const int lt = balanced_threads(ctx, n, ctx->tuning.leaf_threads);
+        const u64 per = (u64)PB_BALANCED_K * (u64)lt;
         const unsigned g = (unsigned)((n + per - 1) / per);
-        switch (ctx->tuning.leaf_threads) {
+        switch (lt) {
         case 128: k_leaf2_balanced<C, S, 128><<<g, 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         case 512: k_leaf2_balanced<C, S, 512><<<g, 512, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         case 1024: k_leaf2_balanced<C, S, 1024><<<g, 1024, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
@@ -682,14 +694,14 @@ int bfs_tt_roots(pb_ctx *ctx, const Board *rb, const uint8_t *rs, const Hash128 
     if (ctx->timing) PB_CUDA(cudaEventRecord(ctx->ev[1], s));
     if (n > 0 && leaf_mode(ctx) >= 1 && ctx->tuning.tt_leaf == 2) {
         PB_CUDA(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s));
-        int rc2 = launch_tt_fill(ctx, c, strict, leaf_mode(ctx), cur_b, cur_s, cur_h, epi, emv, n, n_par,
-                                 ctx->dtt.at(2), leafcnt, cursor);
+        int rc2 = launch_tt_fill(ctx, c, strict, std::min(leaf_mode(ctx), 2), cur_b, cur_s, cur_h, epi, emv, n,
+                                 n_par, ctx->dtt.at(2), leafcnt, cursor);
         if (rc2 != PB_OK) return rc2;
         stats.kernels += 1;
     } else if (n > 0) {
         TTView tv = ctx->dtt.at(2);
         unsigned g = grid_for(n, PB_LEAF_THREADS);
-        const int mode = leaf_mode(ctx);
+        const int mode = std::min(leaf_mode(ctx), 2);
 #define PB_TT_LEAF(CC, SS)                                                                                     \
     if (mode == 2)                                                                                             \
         k_leaf2_tt<CC, SS, 2><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_h, epi, emv, n, n_par, tv,        \
@@ -967,8 +979,19 @@ int bfs_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth,
         } else {
             unsigned g = grid_for(ne, PB_LEAF_THREADS);
             const int mode = leaf_mode(ctx);
+            const int bt = balanced_threads(ctx, ne, 1024);
+            const unsigned gb = (unsigned)((ne + (u64)PB_BALANCED_K * bt - 1) / ((u64)PB_BALANCED_K * bt));
 #define PB_ROOTED_LEAF(CC, SS)                                                                                   \
-    if (mode == 2)                                                                                               \
+    if (mode == 3 && bt == 1024)                                                                                 \
+        k_leaf2_rooted_balanced<CC, SS, 1024><<<gb, 1024, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc,  \
+                                                                  ctx->d_counter);                               \
+    else if (mode == 3 && bt == 512)                                                                             \
+        k_leaf2_rooted_balanced<CC, SS, 512><<<gb, 512, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc,    \
+                                                                ctx->d_counter);                                 \
+    else if (mode == 3)                                                                                          \
+        k_leaf2_rooted_balanced<CC, SS, 256><<<gb, 256, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc,    \
+                                                                ctx->d_counter);                                 \
+    else if (mode == 2)                                                                                          \
         k_leaf2_rooted<CC, SS, 2><<<g, PB_LEAF_THREADS, 0, s>>>(cur_b, cur_s, cur_r, epi, emv, ne, n_par, rc,    \
                                                                 ctx->d_counter);                                 \
     else if (mode == 1)                                                                                          \
@@ -1076,6 +1099,22 @@ void launch_leaf_grid_t(cudaStream_t s, const Board *b, const uint8_t *st, const
 }
 // Leaf of a planned batch: the grid leaf over the planned capacity, or the
 // persistent work-queue leaf (queue).
+// Balanced leaf over a planned level: the grid covers the capacity.
+template <int C, bool S>
+void launch_leaf_balanced_dev(cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r,
+                              const u32 *pi, const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev,
+                              u64 npar_cap, unsigned long long *rc, unsigned long long *counter, u32 *err)
+{
+    const bool big = cap >= (u64)PB_BALANCED_K * 1024u * 8u * (u64)sms;
+    const u64 per = (u64)PB_BALANCED_K * (big ? 1024u : 256u);
+    const unsigned grid = (unsigned)std::max<u64>((cap + per - 1) / per, 1);
+    if (big)
+        k_leaf2_rooted_balanced_dev<C, S, 1024><<<grid, 1024, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap,
+                                                                      rc, counter, err);
+    else
+        k_leaf2_rooted_balanced_dev<C, S, 256><<<grid, 256, 0, s>>>(b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap,
+                                                                    rc, counter, err);
+}
 template <int C, bool S, int MODE>
 void launch_leaf_planned_t(bool queue, cudaStream_t s, int sms, const Board *b, const uint8_t *st, const u32 *r,
                            const u32 *pi, const uint16_t *mv, const u64 *n_dev, u64 cap, const u64 *npar_dev,
@@ -1094,7 +1133,9 @@ void launch_leaf_queue(int mode, bool queue, cudaStream_t s, int sms, const Boar
                        const u64 *npar_dev, u64 npar_cap, unsigned long long *cursor, unsigned long long *rc,
                        unsigned long long *counter, u32 *err)
 {
-    if (mode == 2)
+    if (mode == 3 && !queue)
+        launch_leaf_balanced_dev<C, S>(s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, rc, counter, err);
+    else if (mode >= 2)
         launch_leaf_planned_t<C, S, 2>(queue, s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc,
                                        counter, err);
     else if (mode == 1)

@@ -593,78 +593,6 @@ __global__ void __launch_bounds__(T, PB_LISTED_WARPS_PER_SM * 32 / T) k_leaf2_li
     }
 }
 
-// Ranked leaf with work balanced across the CTA's warps (leaf kernel 6).  In
-// the ranked leaves warp 0 gets the CTA's lightest children and the last warp
-// the heaviest; a warp that finishes early keeps its registers until its
-// CTA ends, so on the bench position only 26.6 of the 32 resident warps were
-// active on average.  Here each thread makes K = PB_BALANCED_K children (the
-// CTA covers KT edges) and counts their moves; the 4T children are ranked by move count
-// and cut into 32-child chunks in rank order; chunk j is paired with chunk
-// NCH - 1 - j (a light and a heavy one) and pair j goes to warp j % W, so
-// every warp gets about the same work while the lanes of a chunk still have
-// similar loop lengths.  Only edge indices pass through shared memory (4 B
-// per child): each lane remakes its child from the parent and the move, then
-// generates its moves and counts the grandchildren with listed pieces.
-#ifndef PB_BALANCED_K
-#define PB_BALANCED_K 4  // children per thread of k_leaf2_balanced
-#endif
-template <int C, bool STRICT, int T>
-__global__ void __launch_bounds__(T, 1024 / T) k_leaf2_balanced(const Board *__restrict__ pboards,
-                                                                const uint8_t *__restrict__ pstates,
-                                                                const u32 *__restrict__ pidx,
-                                                                const uint16_t *__restrict__ moves, u64 n,
-                                                                u64 nparents, unsigned long long *__restrict__ counter)
-{
-    constexpr int K = PB_BALANCED_K;
-    constexpr int W = T / 32;
-    constexpr int NCH = K * T / 32;
-    static_assert(K % 2 == 0 && NCH == K * W, "K/2 chunk pairs per warp");
-    constexpr u32 NONE = 0xFFFFFFFFu;
-    __shared__ u32 s_edge[K * T];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const u64 first = (u64)blockIdx.x * (K * T);
-    u32 key[K], rank[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        const u64 i = first + (u64)k * T + tid;
-        key[k] = 0;
-        if (i < n && pidx[i] < nparents) {
-            const u32 p = pidx[i];
-            Board b = load_board(pboards + p);
-            u32 st = pstates[p];
-            make_move<C>(b, st, moves[i]);
-            key[k] = 1 + min(count_moves<1 - C, true>(b, st), 254u);
-        }
-    }
-    cta_rank_u8<T, K>(key, rank);
-#pragma unroll
-    for (int k = 0; k < K; k++) s_edge[rank[k]] = key[k] ? (u32)(first + (u64)k * T + tid) : NONE;
-    __syncthreads();
-    u32 total = 0, counted = 0;
-    for (int q = 0; q < K; q++) {
-        const int pair = warp + (q >> 1) * W;
-        const int chunk = (q & 1) ? NCH - 1 - pair : pair;
-        const u32 e = s_edge[chunk * 32 + lane];
-        if (e != NONE) {
-            const u32 p = pidx[e];
-            Board b = load_board(pboards + p);
-            u32 st = pstates[p];
-            make_move<C>(b, st, moves[e]);
-            uint16_t mv[MAX_MOVES];
-            ArraySink sink{mv, 0};
-            gen_moves<1 - C>(b, st, sink);
-            total += grandchild_counts<C, STRICT, true, T>(b, st, mv, sink.n);
-            counted += sink.n;
-        }
-    }
-    total = __reduce_add_sync(0xffffffffu, total);
-    counted = __reduce_add_sync(0xffffffffu, counted);
-    if (lane == 0 && counted) {
-        atomicAdd(counter, (unsigned long long)total);
-        atomicAdd(counter + 1, (unsigned long long)counted);
-    }
-}
-
 // ---------------------------------------------------------------- cooperative leaf
 // Fused two-ply leaf with the grandchild work spread over the whole CTA.
 //
@@ -854,6 +782,107 @@ __device__ __forceinline__ void add_by_key(unsigned long long *out, u32 key, u32
     if ((int)(threadIdx.x & 31) == __ffs(peers) - 1 && total) atomicAdd(out + key, (unsigned long long)total);
 }
 
+// Ranked leaf with work balanced across the CTA's warps (leaf kernel 6).  In
+// the ranked leaves warp 0 gets the CTA's lightest children and the last warp
+// the heaviest; a warp that finishes early keeps its registers until its
+// CTA ends, so on the bench position only 26.6 of the 32 resident warps were
+// active on average.  Here each thread makes K = PB_BALANCED_K children (the
+// CTA covers KT edges) and counts their moves; the 4T children are ranked by move count
+// and cut into 32-child chunks in rank order; chunk j is paired with chunk
+// NCH - 1 - j (a light and a heavy one) and pair j goes to warp j % W, so
+// every warp gets about the same work while the lanes of a chunk still have
+// similar loop lengths.  Only edge indices pass through shared memory (4 B
+// per child): each lane remakes its child from the parent and the move, then
+// generates its moves and counts the grandchildren with listed pieces.
+#ifndef PB_BALANCED_K
+#define PB_BALANCED_K 4  // children per thread of k_leaf2_balanced
+#endif
+// With ROOTED every edge's count goes to its root's counter (batched roots).
+template <int C, bool STRICT, int T, bool ROOTED>
+__device__ __forceinline__ void leaf2_balanced_cta(const Board *__restrict__ pboards,
+                                                   const uint8_t *__restrict__ pstates,
+                                                   const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
+                                                   const uint16_t *__restrict__ moves, u64 n, u64 nparents,
+                                                   unsigned long long *__restrict__ root_counts,
+                                                   unsigned long long *__restrict__ counter)
+{
+    constexpr int K = PB_BALANCED_K;
+    constexpr int W = T / 32;
+    constexpr int NCH = K * T / 32;
+    static_assert(K % 2 == 0 && NCH == K * W, "K/2 chunk pairs per warp");
+    constexpr u32 NONE = 0xFFFFFFFFu;
+    __shared__ u32 s_edge[K * T];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u64 first = (u64)blockIdx.x * (K * T);
+    u32 key[K], rank[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const u64 i = first + (u64)k * T + tid;
+        key[k] = 0;
+        if (i < n && pidx[i] < nparents) {
+            const u32 p = pidx[i];
+            Board b = load_board(pboards + p);
+            u32 st = pstates[p];
+            make_move<C>(b, st, moves[i]);
+            key[k] = 1 + min(count_moves<1 - C, true>(b, st), 254u);
+        }
+    }
+    cta_rank_u8<T, K>(key, rank);
+#pragma unroll
+    for (int k = 0; k < K; k++) s_edge[rank[k]] = key[k] ? (u32)(first + (u64)k * T + tid) : NONE;
+    __syncthreads();
+    u32 total = 0, counted = 0;
+    for (int q = 0; q < K; q++) {
+        const int pair = warp + (q >> 1) * W;
+        const int chunk = (q & 1) ? NCH - 1 - pair : pair;
+        const u32 e = s_edge[chunk * 32 + lane];
+        u32 t = 0, root = 0;
+        if (e != NONE) {
+            const u32 p = pidx[e];
+            if (ROOTED) root = proot[p];
+            Board b = load_board(pboards + p);
+            u32 st = pstates[p];
+            make_move<C>(b, st, moves[e]);
+            uint16_t mv[MAX_MOVES];
+            ArraySink sink{mv, 0};
+            gen_moves<1 - C>(b, st, sink);
+            t = grandchild_counts<C, STRICT, true, T>(b, st, mv, sink.n);
+            counted += sink.n;
+        }
+        if (ROOTED)
+            add_by_key(root_counts, root, t, e != NONE);
+        else
+            total += t;
+    }
+    counted = __reduce_add_sync(0xffffffffu, counted);
+    if (!ROOTED) total = __reduce_add_sync(0xffffffffu, total);
+    if (lane == 0 && counted) {
+        if (!ROOTED) atomicAdd(counter, (unsigned long long)total);
+        atomicAdd(counter + 1, (unsigned long long)counted);
+    }
+}
+
+template <int C, bool STRICT, int T>
+__global__ void __launch_bounds__(T, 1024 / T) k_leaf2_balanced(const Board *__restrict__ pboards,
+                                                                const uint8_t *__restrict__ pstates,
+                                                                const u32 *__restrict__ pidx,
+                                                                const uint16_t *__restrict__ moves, u64 n,
+                                                                u64 nparents, unsigned long long *__restrict__ counter)
+{
+    leaf2_balanced_cta<C, STRICT, T, false>(pboards, pstates, nullptr, pidx, moves, n, nparents, nullptr, counter);
+}
+
+// The balanced leaf over batched roots (leaf mode 3 of the batched paths).
+template <int C, bool STRICT, int T>
+__global__ void __launch_bounds__(T, 1024 / T)
+    k_leaf2_rooted_balanced(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                            const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
+                            const uint16_t *__restrict__ moves, u64 n, u64 nparents,
+                            unsigned long long *__restrict__ root_counts, unsigned long long *__restrict__ counter)
+{
+    leaf2_balanced_cta<C, STRICT, T, true>(pboards, pstates, proot, pidx, moves, n, nparents, root_counts, counter);
+}
+
 // Children of a CTA (one per thread) handed to threads in order of their
 // move counts, as in k_leaf2_sorted, carrying their root index along.  On
 // return thread t holds the child of rank t; `valid` says whether it has one.
@@ -906,7 +935,7 @@ __device__ __forceinline__ void leaf2_rooted_cta(const Board *__restrict__ pboar
         uint16_t mv[MAX_MOVES];
         ArraySink sink{mv, 0};
         gen_moves<1 - C>(b, st, sink);
-        total = grandchild_counts<C, STRICT, MODE == 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
+        total = grandchild_counts<C, STRICT, MODE >= 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
         counted = sink.n;
     }
     add_by_key(root_counts, root, total, valid);
@@ -985,6 +1014,24 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
     if ((u64)blockIdx.x * blockDim.x >= n) return;
     const u64 npar = min(*npar_dev, npar_cap);
     leaf2_rooted_cta<C, STRICT, MODE>(pboards, pstates, proot, pidx, moves, n, npar, root_counts, counter);
+}
+
+// The balanced rooted leaf with the level sizes in device memory (planned
+// graphs): the grid covers the planned capacity; CTAs past the level's
+// actual size leave at once.
+template <int C, bool STRICT, int T>
+__global__ void __launch_bounds__(T, 1024 / T)
+    k_leaf2_rooted_balanced_dev(const Board *__restrict__ pboards, const uint8_t *__restrict__ pstates,
+                                const u32 *__restrict__ proot, const u32 *__restrict__ pidx,
+                                const uint16_t *__restrict__ moves, const u64 *__restrict__ n_dev, u64 cap,
+                                const u64 *__restrict__ npar_dev, u64 npar_cap,
+                                unsigned long long *__restrict__ root_counts, unsigned long long *__restrict__ counter,
+                                u32 *__restrict__ err)
+{
+    const u64 n = dev_size(n_dev, cap, err);
+    if ((u64)blockIdx.x * (PB_BALANCED_K * T) >= n) return;
+    const u64 npar = min(*npar_dev, npar_cap);
+    leaf2_balanced_cta<C, STRICT, T, true>(pboards, pstates, proot, pidx, moves, n, npar, root_counts, counter);
 }
 
 // Scan with a device-resident length (grid = tiles of the capacity; surplus
@@ -1136,7 +1183,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
             uint16_t mv[MAX_MOVES];
             ArraySink sink{mv, 0};
             gen_moves<1 - C>(b, st, sink);
-            total = grandchild_counts<C, STRICT, MODE == 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
+            total = grandchild_counts<C, STRICT, MODE >= 2, PB_LEAF_THREADS>(b, st, mv, sink.n);
             counted += sink.n;
         }
         add_by_key(root_counts, root, total, valid);

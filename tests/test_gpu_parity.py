@@ -248,9 +248,9 @@ def test_edge_depths_and_terminal_positions(gpu_engine, oracle):
 
 def test_batched_leaf_ranked_and_unranked_agree():
     """The batched leaf with and without ranking each CTA's children by move
-    count, and ranked with listed pieces (leaf_kernel 4 / 1 / 5), on uneven
-    roots, both colours to move; also the planned batches' grid and queue
-    leaves with listed pieces."""
+    count, ranked with listed pieces, and balanced across the warps
+    (leaf_kernel 4 / 1 / 5 / 6), on uneven roots, both colours to move; also
+    the planned batches' grid and queue leaves with kernels 5 and 6."""
     eng = pg.Engine(device=0, use_tt=False, arena_bytes=2 << 30)
     roots = pg.uneven_roots(192, 6, 40, seed=23)
     depths = [2 + (i % 4) for i in range(len(roots))]
@@ -260,13 +260,22 @@ def test_batched_leaf_ranked_and_unranked_agree():
     plain = eng.perft_batch(roots, depths)
     eng.set_tuning(leaf_kernel=5)
     listed = eng.perft_batch(roots, depths)
-    assert ranked == plain == listed
+    eng.set_tuning(leaf_kernel=6)
+    balanced = eng.perft_batch(roots, depths)
+    assert ranked == plain == listed == balanced
     assert ranked == [eng.perft_position(r, d) for r, d in zip(roots, depths)]
     eng.mlp_init(seed=3, out_bias=[4.5, 9.5, 14.5, 19.0])
-    for planned_leaf in (1, 2):
-        eng.set_tuning(planned_leaf=planned_leaf)
-        got, _ = eng.perft_batch_planned(roots, depths)
-        assert list(got) == ranked, planned_leaf
+    for leaf_kernel in (5, 6):
+        for planned_leaf in (1, 2):
+            eng.set_tuning(leaf_kernel=leaf_kernel, planned_leaf=planned_leaf)
+            got, _ = eng.perft_batch_planned(roots, depths)
+            assert list(got) == ranked, (leaf_kernel, planned_leaf)
+    # a batch big enough for 1024-thread balanced CTAs (more than 8 per SM)
+    big = pg.uneven_roots(2048, 6, 30, seed=29)
+    eng.set_tuning(leaf_kernel=6)
+    b6 = eng.perft_batch(big, [5] * len(big))
+    eng.set_tuning(leaf_kernel=1)
+    assert b6 == eng.perft_batch(big, [5] * len(big))
     eng.close()
 
 
