@@ -196,6 +196,13 @@ inline int balanced_threads(const pb_ctx *ctx, u64 n, int tuned)
     while (t > 256 && n < (u64)PB_BALANCED_K * (u64)t * 8u * (u64)ctx->num_sms) t /= 2;
     return t;
 }
+// Below this many edges even 256-thread balanced CTAs would not give every SM
+// 8 of them: such small leaves run one edge per thread (the listed leaf) so
+// the launch still covers the GPU (one perft-5 root has about 3e4 edges).
+inline bool balanced_fits(const pb_ctx *ctx, u64 n)
+{
+    return n >= (u64)PB_BALANCED_K * 256u * 8u * (u64)ctx->num_sms;
+}
 
 // NVTX range for profilers (header-only NVTX v3: free unless a tool attaches):
 // marks each BFS pass, level and leaf launch on the host timeline, so a
@@ -226,7 +233,7 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
         PB_CUDA(cudaGetLastError());
         return PB_OK;
     }
-    if (ctx->tuning.leaf_kernel == 6) {
+    if (ctx->tuning.leaf_kernel == 6 && balanced_fits(ctx, n)) {
         // PB_BALANCED_K edges per thread
         const int lt = balanced_threads(ctx, n, ctx->tuning.leaf_threads);
         const u64 per = (u64)PB_BALANCED_K * (u64)lt;
@@ -240,8 +247,8 @@ int launch_leaf_t(pb_ctx *ctx, const Board *b, const uint8_t *st, const u32 *pi,
         PB_CUDA(cudaGetLastError());
         return PB_OK;
     }
-    if (ctx->tuning.leaf_kernel == 5) {
-        switch (ctx->tuning.leaf_threads) {
+    if (ctx->tuning.leaf_kernel == 5 || ctx->tuning.leaf_kernel == 6) {
+        switch (ctx->tuning.leaf_kernel == 6 ? 256 : ctx->tuning.leaf_threads) {
         case 128: k_leaf2_listed<C, S, 128><<<grid_for(n, 128), 128, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         case 512: k_leaf2_listed<C, S, 512><<<grid_for(n, 512), 512, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
         default: k_leaf2_listed<C, S, 256><<<grid_for(n, 256), 256, 0, s>>>(b, st, pi, mv, n, npar, ctx->d_counter); break;
@@ -978,7 +985,7 @@ int bfs_batch(pb_ctx *ctx, const Board *rb, const uint8_t *rs, u64 n, int depth,
             }
         } else {
             unsigned g = grid_for(ne, PB_LEAF_THREADS);
-            const int mode = leaf_mode(ctx);
+            const int mode = (leaf_mode(ctx) == 3 && !balanced_fits(ctx, ne)) ? 2 : leaf_mode(ctx);
             const int bt = balanced_threads(ctx, ne, 1024);
             const unsigned gb = (unsigned)((ne + (u64)PB_BALANCED_K * bt - 1) / ((u64)PB_BALANCED_K * bt));
 #define PB_ROOTED_LEAF(CC, SS)                                                                                   \
@@ -1133,7 +1140,7 @@ void launch_leaf_queue(int mode, bool queue, cudaStream_t s, int sms, const Boar
                        const u64 *npar_dev, u64 npar_cap, unsigned long long *cursor, unsigned long long *rc,
                        unsigned long long *counter, u32 *err)
 {
-    if (mode == 3 && !queue)
+    if (mode == 3 && !queue && cap >= (u64)PB_BALANCED_K * 256u * 8u * (u64)sms)
         launch_leaf_balanced_dev<C, S>(s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, rc, counter, err);
     else if (mode >= 2)
         launch_leaf_planned_t<C, S, 2>(queue, s, sms, b, st, r, pi, mv, n_dev, cap, npar_dev, npar_cap, cursor, rc,
