@@ -250,11 +250,13 @@ int pb_selftest_wait_timeout(pb_ctx *ctx, uint32_t *device_error, double *second
 
 /* Race self-test of the device tables (no reference counterpart; the
  * reference relies on the same kind of XOR lock, tt.h:9-14,49-57): all the
- * GPU's threads store and probe 8192 keys in a 1024-slot table of the 16-byte
- * (deep = 0) or 32-byte (deep = 1) format at once.  *bad = probes that
- * reported a hit with a count that is not the key's own (must be 0),
- * *hits = probes that hit. */
-int pb_selftest_tt_race(pb_ctx *ctx, int deep, uint64_t *bad, uint64_t *hits);
+ * GPU's threads store and probe 8192 keys at once in a 1024-slot table of the
+ * 16-byte (mode 0) or 32-byte (mode 1) format, or (mode 2) in a 2^24-slot
+ * 16-byte table, the smallest the engine builds in that format, with the
+ * keys chosen to fall into 8 of its slots.  *bad = probes that reported a
+ * hit with a count that is not the key's own (must be 0), *hits = probes
+ * that hit. */
+int pb_selftest_tt_race(pb_ctx *ctx, int mode, uint64_t *bad, uint64_t *hits);
 
 /* Learned scheduler network (no reference counterpart): 781 binary inputs
  * (12x64 piece-square, side to move, 4 castle rights, 8 en-passant files) ->

@@ -536,11 +536,13 @@ class Engine:
         """The staged generation kernel on caller-owned device buffers (tests)."""
         self._check(lib.pb_dev_generate(self._h, d_boards, d_states, color, d_offs, d_total, n, d_moves, d_pidx))
 
-    def selftest_tt_race(self, deep: bool):
-        """(wrong hits, hits) of the device-table race self-test."""
+    def selftest_tt_race(self, mode: int):
+        """(wrong hits, hits) of the device-table race self-test: mode 0 =
+        1024-slot 16-byte table, 1 = 1024-slot 32-byte table, 2 = 2^24-slot
+        16-byte table with the keys packed into 8 slots."""
         bad = ctypes.c_uint64()
         hits = ctypes.c_uint64()
-        self._check(lib.pb_selftest_tt_race(self._h, int(deep), ctypes.byref(bad), ctypes.byref(hits)))
+        self._check(lib.pb_selftest_tt_race(self._h, int(mode), ctypes.byref(bad), ctypes.byref(hits)))
         return bad.value, hits.value
 
     def selftest_wait_timeout(self):

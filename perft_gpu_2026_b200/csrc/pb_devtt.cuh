@@ -130,14 +130,25 @@ __device__ __forceinline__ Hash128 race_key(u32 k)
     return h;
 }
 __device__ __forceinline__ u64 race_count(const Hash128 &h) { return (h.lo ^ (h.hi >> 7)) & 0xFFFFFULL; }
-__global__ void k_tt_race(TTView t, u32 nkeys, u32 iters, unsigned long long *bad, unsigned long long *hits)
+// With `packed`, bits 40..42 of the key's lo are the key's number mod 8 and
+// the bits above are zero, so in a table of 2^24 slots (slot = lo >> 40) all
+// keys fall into 8 slots: the shallow format at the size the engine allows,
+// under the same contention as the small table.
+__device__ __forceinline__ Hash128 race_key_in(u32 k, bool packed)
+{
+    Hash128 h = race_key(k);
+    if (packed) h.lo = (h.lo & ((1ULL << 40) - 1)) | ((u64)(k & 7u) << 40);
+    return h;
+}
+__global__ void k_tt_race(TTView t, u32 nkeys, u32 iters, u32 packed, unsigned long long *bad,
+                          unsigned long long *hits)
 {
     const u32 tid = blockIdx.x * blockDim.x + threadIdx.x;
     u64 wrong = 0, seen = 0;
     for (u32 it = 0; it < iters; it++) {
-        const Hash128 a = race_key((tid * 2654435761u + it * 40503u) % nkeys);
+        const Hash128 a = race_key_in((tid * 2654435761u + it * 40503u) % nkeys, packed != 0);
         tt_store(t, a, race_count(a));
-        const Hash128 b = race_key((tid * 97u + it * 7919u + 1u) % nkeys);
+        const Hash128 b = race_key_in((tid * 97u + it * 7919u + 1u) % nkeys, packed != 0);
         u64 c;
         if (tt_probe(t, b, &c)) {
             seen++;

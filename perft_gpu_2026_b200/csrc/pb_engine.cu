@@ -2312,12 +2312,15 @@ int pb_dev_generate(pb_ctx *ctx, const void *d_boards, const uint8_t *d_states, 
     return finish_test_launch(ctx, "generation kernel reported a device error");
 }
 
-int pb_selftest_tt_race(pb_ctx *ctx, int deep, uint64_t *bad, uint64_t *hits)
+int pb_selftest_tt_race(pb_ctx *ctx, int mode, uint64_t *bad, uint64_t *hits)
 {
-    if (!ctx || !ctx->gpu || !bad || !hits) return PB_ERR_ARG;
+    if (!ctx || !ctx->gpu || !bad || !hits || mode < 0 || mode > 2) return PB_ERR_ARG;
     PB_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
-    const u64 slots = 1024;  // far fewer slots than keys: constant collisions
+    const bool deep = mode == 1, packed = mode == 2;
+    // far fewer slots than keys (constant collisions); mode 2: the smallest
+    // shallow table the engine builds, with every key packed into 8 slots
+    const u64 slots = packed ? (1ULL << 24) : 1024;
     Arena ar{ctx->arena, ctx->arena_bytes};
     u64 *entries = ar.take<u64>(slots * (deep ? 4 : 2));
     unsigned long long *cnt = ar.take<unsigned long long>(2);
@@ -2325,7 +2328,7 @@ int pb_selftest_tt_race(pb_ctx *ctx, int deep, uint64_t *bad, uint64_t *hits)
     PB_CUDA(cudaMemsetAsync(entries, 0, slots * (deep ? 32 : 16), s));
     PB_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), s));
     const TTView t{entries, slots, deep ? TT_DEEP : TT_SHALLOW, 0};
-    k_tt_race<<<4 * ctx->num_sms, 256, 0, s>>>(t, 8192, 64, cnt, cnt + 1);
+    k_tt_race<<<4 * ctx->num_sms, 256, 0, s>>>(t, 8192, 64, packed ? 1u : 0u, cnt, cnt + 1);
     PB_CUDA(cudaGetLastError());
     PB_CUDA(cudaMemcpyAsync(ctx->h_pinned, cnt, 2 * sizeof(u64), cudaMemcpyDeviceToHost, s));
     PB_CUDA(cudaStreamSynchronize(s));
