@@ -319,13 +319,14 @@ def positions_section(pg, eng, reps):
     seed 2), perft 5 each, three ways through the public API (roots in host
     memory, counts read back, host wall clock): one plain call per root, one
     count-then-allocate batched call, and the learned planner (the network
-    scheduler_section trained).  Also the planner at perft 3 and 4 of the same
-    roots, where each batch's per-level host round trips are a larger share.
-    All modes must agree."""
+    scheduler_section trained).  The roots are held as one packed pb_pos array
+    (pack_positions, the C ABI's batch format) by every mode.  Also the planner
+    at perft 3 and 4 of the same roots, where each batch's per-level host round
+    trips are a larger share.  All modes must agree."""
     import numpy as np
     from perft_gpu_2026_b200 import scheduler
 
-    roots = pg.uneven_roots(4096, 6, 40, seed=2)
+    roots = pg.pack_positions(pg.uneven_roots(4096, 6, 40, seed=2))
     depths = [5] * len(roots)
     truth = np.log2(1.0 + scheduler.label(eng, roots))
     mae = np.abs(eng.mlp_predict(roots) - truth).mean(0).tolist()
@@ -336,13 +337,13 @@ def positions_section(pg, eng, reps):
     n = len(roots)
     shallow = {}
     for d in (3, 4):
-        b, tb = _timed(lambda: eng.perft_batch(roots, [d] * n), 5)
-        (l, _), tl = _timed(lambda: eng.perft_batch_planned(roots, [d] * n), 5)
+        b, tb = _timed(lambda: eng.perft_batch(roots, d), 5)
+        (l, _), tl = _timed(lambda: eng.perft_batch_planned(roots, d), 5)
         assert b == list(l)
         shallow[f"perft{d}"] = {"batched": n / tb, "learned": n / tl, "learned_vs_batched": tb / tl}
     return {"workload": "4096 uneven roots (6..40-ply playouts, seed 2), perft 5 each, no TT",
-            "unit": "positions/s", "timing": "host wall clock around the public call, best of "
-                                             f"{reps} after one warm-up",
+            "unit": "positions/s", "timing": "host wall clock around the public call, roots in one packed "
+                                             f"pb_pos array, best of {reps} after one warm-up",
             "nodes": int(sum(plain)), "plain": n / t_plain, "batched": n / t_batched, "learned": n / t_learned,
             "learned_vs_plain": t_plain / t_learned, "batched_vs_plain": t_plain / t_batched,
             "learned_vs_batched": t_batched / t_learned,

@@ -274,6 +274,17 @@ int pb_mlp_train(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n, in
                  uint64_t seed, float *final_loss);
 int pb_mlp_predict(pb_ctx *ctx, const pb_pos *pos, int n, float *out);
 
+/* Self-test of the network's tensor-core GEMM (tcgen05, BF16 operands, FP32
+ * accumulation) on the context's GPU: c[M x N] (row-major) = A * B, where
+ * element (m, k) of A is a[m*K + k], or with ta a[k*M + m], and element
+ * (k, n) of B is b[k*N + n], or with tb b[n*K + k]; a and b hold BF16 bit
+ * patterns.  M a multiple of 8, N of 128, K of 64 (else PB_ERR_ARG).  With
+ * reps > 0 the product then runs reps more times between two CUDA events on
+ * the context's stream and *ms = their mean duration.  No reference
+ * counterpart. */
+int pb_selftest_gemm(pb_ctx *ctx, int ta, int tb, int M, int N, int K, const uint16_t *a, const uint16_t *b,
+                     float *c, int reps, double *ms);
+
 /* Learned batch planner (no reference counterpart): like pb_perft_batch, but
  * the network's predictions size every BFS level up front, bin-pack the roots
  * into batches that fit the arena and split roots too large for one batch;

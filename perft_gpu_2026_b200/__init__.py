@@ -156,6 +156,9 @@ def _load() -> ctypes.CDLL:
         "pb_dev_scan": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
         "pb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_uint32), P(ctypes.c_double)]),
         "pb_selftest_tt_race": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, P(ctypes.c_uint64), P(ctypes.c_uint64)]),
+        "pb_selftest_gemm": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, P(ctypes.c_uint16), P(ctypes.c_uint16), P(ctypes.c_float),
+                                            ctypes.c_int, P(ctypes.c_double)]),
         "pb_dev_expand": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p]),
@@ -286,14 +289,36 @@ def random_playout(seed_state: int, plies: int) -> Tuple[Pos, int, int]:
     return p, n, st.value
 
 
-def random_playouts(seed: int, n: int, min_plies: int, max_plies: int) -> List[Pos]:
+def random_playouts(seed: int, n: int, min_plies: int, max_plies: int, packed: bool = False):
     """n playouts (threaded in the library); position i's generator state is
-    the i-th splitmix64 draw of `seed`, its length uniform in [min, max]."""
+    the i-th splitmix64 draw of `seed`, its length uniform in [min, max].
+    A list of Pos, or with packed=True the packed array (pack_positions)."""
     arr = (Pos * n)()
     rc = lib.pb_random_playouts(seed, n, min_plies, max_plies, arr, None)
     if rc != PB_OK:
         raise PerftError(rc, "pb_random_playouts failed")
-    return list(arr)
+    return arr if packed else list(arr)
+
+
+def pack_positions(roots) -> ctypes.Array:
+    """Positions as one contiguous pb_pos array, the batch format of the C
+    ABI (pb_perft_batch, pb_perft_batch_planned, pb_mlp_predict).  A packed
+    array is returned as it is; a sequence of Pos is copied once.  The batch
+    methods accept either; passing the packed array spares the copy (about
+    0.3 us per position in CPython) on every call."""
+    if isinstance(roots, ctypes.Array) and roots._type_ is Pos:
+        return roots
+    return (Pos * len(roots))(*roots)
+
+
+def _c_ints(values, n: int):
+    """Per-position ints (or one int for all) as a contiguous C int array."""
+    import numpy as np
+
+    a = np.full(n, values, dtype=np.intc) if np.ndim(values) == 0 else np.ascontiguousarray(values, dtype=np.intc)
+    if a.shape != (n,):
+        raise ValueError(f"expected {n} values, got shape {a.shape}")
+    return a
 
 
 def splitmix64(state: int) -> Tuple[int, int]:
@@ -407,23 +432,35 @@ class Engine:
         self._check(lib.pb_perft_cpu(self._h, ctypes.byref(p), depth, ctypes.byref(out)))
         return out.value
 
-    def perft_batch_planned(self, roots: Sequence[Pos], depths: Sequence[int]):
-        """Learned-planner batch: returns (counts, PlanStats)."""
-        n = len(roots)
-        arr = (Pos * n)(*roots)
-        d = (ctypes.c_int * n)(*depths)
-        out = (ctypes.c_uint64 * n)()
-        st = PlanStats()
-        self._check(lib.pb_perft_batch_planned(self._h, arr, d, n, out, ctypes.byref(st)))
-        return list(out), st
+    def perft_batch_planned(self, roots, depths):
+        """Learned-planner batch: returns (counts, PlanStats).  roots: a
+        sequence of Pos or a packed array (pack_positions); depths: one int
+        per root, or one int for all."""
+        import numpy as np
 
-    def perft_batch(self, roots: Sequence[Pos], depths: Sequence[int]) -> List[int]:
-        n = len(roots)
-        arr = (Pos * n)(*roots)
-        d = (ctypes.c_int * n)(*depths)
-        out = (ctypes.c_uint64 * n)()
-        self._check(lib.pb_perft_batch(self._h, arr, d, n, out))
-        return list(out)
+        arr = pack_positions(roots)
+        n = len(arr)
+        d = _c_ints(depths, n)
+        out = np.zeros(n, dtype=np.uint64)
+        st = PlanStats()
+        self._check(lib.pb_perft_batch_planned(self._h, arr, d.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n,
+                                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                               ctypes.byref(st)))
+        return out.tolist(), st
+
+    def perft_batch(self, roots, depths) -> List[int]:
+        """Count-then-allocate batch (pb_perft_batch): one count per root.
+        roots: a sequence of Pos or a packed array (pack_positions); depths:
+        one int per root, or one int for all."""
+        import numpy as np
+
+        arr = pack_positions(roots)
+        n = len(arr)
+        d = _c_ints(depths, n)
+        out = np.zeros(n, dtype=np.uint64)
+        self._check(lib.pb_perft_batch(self._h, arr, d.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n,
+                                       out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out.tolist()
 
     def set_timing(self, enable: bool = True) -> None:
         self._check(lib.pb_set_timing(self._h, int(enable)))
@@ -508,8 +545,8 @@ class Engine:
                   seed: int = 7) -> float:
         import numpy as np
 
-        n = len(positions)
-        arr = (Pos * n)(*positions)
+        arr = pack_positions(positions)
+        n = len(arr)
         t = np.ascontiguousarray(targets, dtype=np.float32).reshape(n, 4)
         loss = ctypes.c_float()
         self._check(lib.pb_mlp_train(self._h, arr, t.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, epochs,
@@ -519,8 +556,8 @@ class Engine:
     def mlp_predict(self, positions: Sequence[Pos]):
         import numpy as np
 
-        n = len(positions)
-        arr = (Pos * n)(*positions)
+        arr = pack_positions(positions)
+        n = len(arr)
         out = np.empty((n, 4), dtype=np.float32)
         self._check(lib.pb_mlp_predict(self._h, arr, n, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
@@ -544,6 +581,24 @@ class Engine:
         hits = ctypes.c_uint64()
         self._check(lib.pb_selftest_tt_race(self._h, int(mode), ctypes.byref(bad), ctypes.byref(hits)))
         return bad.value, hits.value
+
+    def selftest_gemm(self, a_bits, b_bits, ta: bool, tb: bool, m: int, n: int, k: int, reps: int = 0):
+        """The network's tensor-core GEMM on BF16 bit patterns (uint16 arrays in
+        the layouts pb_selftest_gemm names); returns C as an (m, n) float32
+        array, or with reps > 0 (C, mean CUDA-event ms of reps more launches)."""
+        import numpy as np
+
+        a = np.ascontiguousarray(a_bits, dtype=np.uint16)
+        b = np.ascontiguousarray(b_bits, dtype=np.uint16)
+        if a.size != m * k or b.size != k * n:
+            raise ValueError("operand sizes do not match m, n, k")
+        c = np.empty((m, n), dtype=np.float32)
+        u16 = ctypes.POINTER(ctypes.c_uint16)
+        ms = ctypes.c_double()
+        self._check(lib.pb_selftest_gemm(self._h, int(ta), int(tb), m, n, k, a.ctypes.data_as(u16),
+                                         b.ctypes.data_as(u16), c.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                         int(reps), ctypes.byref(ms)))
+        return (c, ms.value) if reps > 0 else c
 
     def selftest_wait_timeout(self):
         """(device error word, seconds) of a scan tile whose predecessor never

@@ -1340,30 +1340,35 @@ int run_planned_batch(pb_ctx *ctx, GraphPlan &g, const Board *rb, const uint8_t 
 // ---------------------------------------------------------------- learned planning
 // Level sizes of a depth-d batched perft of one root, from the network's
 // predicted log2(1 + perft(k)), k = 1..4 (geometric beyond 4).
-void predicted_levels(const float *y, int depth, std::vector<double> &e)
+// Number of planned levels of a depth-d batch (depth <= 12).
+constexpr int PLAN_LEVELS = 10;
+inline int plan_levels(int depth) { return std::max(depth - 2, 1); }
+
+void predicted_levels(const float *y, int depth, double *e)
 {
-    e.assign(std::max(depth - 2, 1), 0.0);
     double p[5] = {1, 0, 0, 0, 0};
     for (int k = 1; k <= 4; k++) p[k] = std::max(exp2((double)y[k - 1]) - 1.0, 0.0);
     double bf = p[3] > 0 ? std::max(p[4] / p[3], 1.0) : 30.0;
-    for (int k = 1; k <= (int)e.size(); k++) e[k - 1] = k <= 4 ? p[k] : e[k - 2] * bf;
+    for (int k = 1; k <= plan_levels(depth); k++) e[k - 1] = k <= 4 ? p[k] : e[k - 2] * bf;
 }
 
 // bytes one root's batched levels take: 6 B per edge, 50 B per materialised position
-double level_bytes(const std::vector<double> &e)
+double level_bytes(const double *e, int nlev)
 {
     double b = 0;
-    for (size_t k = 0; k < e.size(); k++) b += e[k] * (6.0 + (k + 1 < e.size() ? 50.0 : 0.0));
+    for (int k = 0; k < nlev; k++) b += e[k] * (6.0 + (k + 1 < nlev ? 50.0 : 0.0));
     return b;
 }
 
+// One root (or a split-off child of one) in the plan; plain data, so the
+// planner's per-root bookkeeping allocates nothing.
 struct PlanItem {
     Board b;
     uint8_t s;
     int depth;
     int owner;
     double bytes;
-    std::vector<double> lv;
+    double lv[PLAN_LEVELS];
 };
 
 }  // namespace
@@ -1390,6 +1395,7 @@ int plan_and_run(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uin
         counts[i] = 0;
     }
     std::vector<PlanItem> ready;
+    ready.reserve(n);
     int guard = 0;
     while (!items.empty() && guard++ < 8) {
         // predict
@@ -1402,7 +1408,7 @@ int plan_and_run(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uin
         for (size_t k = 0; k < items.size(); k++) {
             PlanItem &it = items[k];
             predicted_levels(&y[k * MLP_OUT], it.depth, it.lv);
-            it.bytes = level_bytes(it.lv);
+            it.bytes = level_bytes(it.lv, plan_levels(it.depth));
             if (it.depth >= 4 && it.bytes > budget) {
                 // too big for any batch: split into children one ply down
                 uint16_t mv[MAX_MOVES];
@@ -1429,36 +1435,43 @@ int plan_and_run(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uin
         items.swap(next);
     }
     if (!items.empty()) return fail(ctx, PB_ERR_NOMEM, "planner could not fit a root");
-    // bin-pack per depth: largest first, fill to the budget
-    std::sort(ready.begin(), ready.end(), [](const PlanItem &a, const PlanItem &b) {
-        return a.depth != b.depth ? a.depth < b.depth : a.bytes > b.bytes;
+    // bin-pack per depth: largest first, fill to the budget (an index sort:
+    // the items themselves stay in place)
+    std::vector<u32> order(ready.size());
+    for (size_t k = 0; k < order.size(); k++) order[k] = (u32)k;
+    std::sort(order.begin(), order.end(), [&](u32 a, u32 b) {
+        const PlanItem &x = ready[a], &y2 = ready[b];
+        return x.depth != y2.depth ? x.depth < y2.depth : x.bytes > y2.bytes;
     });
+    std::vector<Board> rb;
+    std::vector<uint8_t> rs;
+    std::vector<u64> out;
     size_t i = 0;
-    while (i < ready.size()) {
-        int d = ready[i].depth;
+    while (i < order.size()) {
+        int d = ready[order[i]].depth;
         size_t j = i;
         double used = 0;
-        while (j < ready.size() && ready[j].depth == d && (j == i || used + ready[j].bytes <= budget) &&
-               j - i < 0xFFFFFFF) {
-            used += ready[j].bytes;
+        while (j < order.size() && ready[order[j]].depth == d &&
+               (j == i || used + ready[order[j]].bytes <= budget) && j - i < 0xFFFFFFF) {
+            used += ready[order[j]].bytes;
             j++;
         }
         u64 m = j - i;
-        std::vector<Board> rb(m);
-        std::vector<uint8_t> rs(m);
-        std::vector<u64> out(m, 0);
+        rb.resize(m);
+        rs.resize(m);
+        out.assign(m, 0);
         for (u64 k = 0; k < m; k++) {
-            rb[k] = ready[i + k].b;
-            rs[k] = ready[i + k].s;
+            rb[k] = ready[order[i + k]].b;
+            rs[k] = ready[order[i + k]].s;
         }
         int rc = PB_OK;
         bool overflow = false;
         if (d <= 1) {
             rc = gpu_batch(ctx, rb.data(), rs.data(), m, d, out.data());
         } else {
-            std::vector<u64> caps(std::max(d - 2, 1), 0);
+            std::vector<u64> caps(plan_levels(d), 0);
             for (u64 k = 0; k < m; k++)
-                for (size_t l = 0; l < caps.size(); l++) caps[l] += (u64)ready[i + k].lv[l];
+                for (size_t l = 0; l < caps.size(); l++) caps[l] += (u64)ready[order[i + k]].lv[l];
             for (auto &c : caps) c = (u64)((double)c * margin) + 4096;
             rc = run_planned_batch(ctx, ctx->graph, rb.data(), rs.data(), m, d, caps, out.data(), &overflow);
             if (rc == PB_OK && overflow) {
@@ -1468,7 +1481,7 @@ int plan_and_run(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uin
             if (ps) ps->graph_batches++;
         }
         if (rc != PB_OK) return rc;
-        for (u64 k = 0; k < m; k++) counts[ready[i + k].owner] += out[k];
+        for (u64 k = 0; k < m; k++) counts[ready[order[i + k]].owner] += out[k];
         if (ps) ps->batches++;
         i = j;
     }
@@ -2432,6 +2445,79 @@ int pb_mlp_set_params(pb_ctx *ctx, const float *in, size_t count)
     return PB_OK;
 }
 
+// The network's GEMM error word (set when a tensor-core wait gave up), read
+// here unless the caller already copied it (*copied): PB_ERR_DEVICE if it
+// was set, and the word is cleared.
+static int mlp_check(pb_ctx *ctx, const u32 *copied = nullptr)
+{
+    u32 e = 0;
+    if (copied)
+        e = *copied;
+    else
+        PB_CUDA(cudaMemcpy(&e, ctx->mlp.err, sizeof(u32), cudaMemcpyDeviceToHost));
+    if (!e) return PB_OK;
+    PB_CUDA(cudaMemset(ctx->mlp.err, 0, sizeof(u32)));
+    return fail(ctx, PB_ERR_DEVICE, "tensor-core GEMM: an mbarrier wait timed out");
+}
+
+int pb_selftest_gemm(pb_ctx *ctx, int ta, int tb, int M, int N, int K, const uint16_t *a, const uint16_t *b,
+                     float *c, int reps, double *ms)
+{
+    if (!ctx || !a || !b || !c || M <= 0 || M % 8 || N <= 0 || N % tc::BN || K <= 0 || K % tc::BK || reps < 0 ||
+        (reps > 0 && !ms))
+        return PB_ERR_ARG;
+    if (!ctx->gpu) return fail(ctx, PB_ERR_NODEVICE, "context has no GPU");
+    PB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const size_t na = (size_t)M * K, nb = (size_t)K * N, nc = (size_t)M * N;
+    __nv_bfloat16 *da = nullptr, *db = nullptr;
+    float *dc = nullptr, *dw = nullptr;
+    u32 *derr = nullptr;
+    int rc = PB_OK;
+    // workspace for as many K splits as the product would use
+    const size_t nw = (size_t)gemm_splits(M, N, K, (size_t)-1) * M * N;
+    cudaError_t e = cudaMalloc(&da, na * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&dw, nw * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&db, nb * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&dc, nc * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(u32));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(da, a, na * 2, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, b, nb * 2, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(u32), s);
+    const int lda = ta ? M : K, ldb = tb ? K : N;
+    auto launch = [&]() {
+        if (ta && tb) return gemm_tc<true, true>(da, lda, db, ldb, dc, N, M, N, K, derr, dw, nw, s);
+        if (ta) return gemm_tc<true, false>(da, lda, db, ldb, dc, N, M, N, K, derr, dw, nw, s);
+        if (tb) return gemm_tc<false, true>(da, lda, db, ldb, dc, N, M, N, K, derr, dw, nw, s);
+        return gemm_tc<false, false>(da, lda, db, ldb, dc, N, M, N, K, derr, dw, nw, s);
+    };
+    if (e == cudaSuccess) e = launch();
+    if (e == cudaSuccess && reps > 0) {
+        // the same product `reps` more times between two events on the stream
+        for (int i = 0; i < 4 && e == cudaSuccess; i++)
+            if (!ctx->ev[i]) e = cudaEventCreate(&ctx->ev[i]);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], s);
+        for (int r = 0; r < reps && e == cudaSuccess; r++) e = launch();
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], s);
+        float t = 0;
+        if (e == cudaSuccess) e = cudaEventSynchronize(ctx->ev[1]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, ctx->ev[0], ctx->ev[1]);
+        if (e == cudaSuccess) *ms = (double)t / reps;
+    }
+    u32 herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c, dc, nc * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(u32), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "gemm self-test");
+    else if (herr) rc = fail(ctx, PB_ERR_DEVICE, "tensor-core GEMM: an mbarrier wait timed out");
+    cudaFree(da);
+    cudaFree(db);
+    cudaFree(dc);
+    cudaFree(dw);
+    cudaFree(derr);
+    return rc;
+}
+
 // Loss and parameter gradients of one batch (n a multiple of 64), no update.
 int pb_mlp_gradients(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n, float *grads, float *loss)
 {
@@ -2448,7 +2534,7 @@ int pb_mlp_gradients(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n
     PB_CUDA(cudaMemcpyAsync(&l, m.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
     PB_CUDA(cudaStreamSynchronize(s));
     if (loss) *loss = l / (float)(n * MLP_OUT);
-    return PB_OK;
+    return mlp_check(ctx);
 }
 
 // Adam training on n examples: `epochs` passes over a fresh shuffle each, in
@@ -2496,7 +2582,7 @@ int pb_mlp_train(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n, in
         if (steps) epoch_loss /= steps;
     }
     if (final_loss) *final_loss = (float)epoch_loss;
-    return PB_OK;
+    return mlp_check(ctx);
 }
 
 // Predicted log2(1 + perft(k)), k = 1..4, for n positions (out: n x 4).
@@ -2517,7 +2603,10 @@ int pb_mlp_predict(pb_ctx *ctx, const pb_pos *pos, int n, float *out)
         PB_CUDA(m.load_positions(tmp.data(), padded, s));
         PB_CUDA(m.forward_backward(padded, false, s));
         PB_CUDA(cudaMemcpyAsync(out + (size_t)b0 * MLP_OUT, m.y, sizeof(float) * MLP_OUT * k, cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaMemcpyAsync(ctx->h_pinned + 3, m.err, sizeof(u32), cudaMemcpyDeviceToHost, s));
         PB_CUDA(cudaStreamSynchronize(s));
+        const u32 e = (u32)ctx->h_pinned[3];
+        if (e) return mlp_check(ctx, &e);
     }
     return PB_OK;
 }

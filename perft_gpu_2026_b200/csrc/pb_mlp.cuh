@@ -8,10 +8,13 @@
 // A position has at most 38 active inputs, so layer 1 is an embedding bag
 // (sum of the active rows of W1), not a GEMM over a 95 %-zero matrix; its
 // weight gradient is a scatter-add into the active rows.  Layer 2 (256x256)
-// runs on the tensor cores with mma.sync m16n8k16 BF16 -> FP32; layer 3
-// (256x4) is a per-sample dot product.
+// and its two backward products run on the tcgen05 tensor cores (BF16
+// operands, FP32 accumulation in tensor memory); layer 3 (256x4) is a
+// per-sample dot product.
 #pragma once
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 #include "pb_core.cuh"
 
@@ -71,86 +74,261 @@ __global__ void k_mlp_layer1(const int16_t *__restrict__ idx, const __nv_bfloat1
 }
 
 // ---------------------------------------------------------------- tensor-core GEMM
-// C[M x N] (FP32) = A[M x K] * B[K x N] with BF16 operands, FP32 accumulation.
-// A is row-major (lda) or, with TA, stored as A^T row-major (element (m,k) at
-// A[k*lda + m]); B likewise with TB.  64x64 block tile, 4 warps (each 32x32 =
-// 2x4 mma tiles of 16x8), K step 16.  M, N multiples of 64, K of 16.
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(128) k_gemm_bf16(const __nv_bfloat16 *__restrict__ A, int lda,
-                                                   const __nv_bfloat16 *__restrict__ B, int ldb,
-                                                   float *__restrict__ C, int ldc, int M, int N, int K,
-                                                   float beta)
-{
-    __shared__ __nv_bfloat16 sA[64][16 + 8];   // [m][k]
-    __shared__ __nv_bfloat16 sB[16][64 + 8];   // [k][n]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    const int g = lane >> 2, t4 = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int a = 0; a < 2; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) acc[a][b][c] = 0.f;
+// C[M x N] (FP32) = A[M x K] * B[K x N], BF16 operands, FP32 accumulation in
+// tensor memory, on the 5th-generation tensor cores (tcgen05).
+//
+// Element (m, k) of A is A[m*lda + k], or with TA A[k*lda + m]; element
+// (k, n) of B is B[k*ldb + n], or with TB B[n*ldb + k].  M a multiple of 8
+// (rows past M read as zero and are not stored), N of 128, K of 64.
+//
+// One CTA of 128 threads per 128 x 128 tile of C (and per K split, below).
+// K advances 64 at a time through two shared-memory stages: all threads
+// stage the next A and B chunks with 16-byte loads and stores while the
+// tensor cores work on the current one.  Each operand keeps the layout it
+// has in global memory, in one of the two canonical no-swizzle layouts of
+// 8 x 16-byte core matrices: K-major (an operand contiguous along K: a
+// core matrix is 8 rows x 8 k; 8-row groups SBO_K = 128 B apart, 8-k groups
+// LBO_K = 2048 B apart) or MN-major (contiguous along M or N: a core matrix
+// is 8 k x 8 rows; 8-row groups SBO_MN = 144 B apart, so that 16 threads
+// storing one k row hit distinct banks, and 8-k groups LBO_MN = 2304 B
+// apart); the instruction descriptor names which.  Thread 0 issues the four
+// 128x128x16 MMAs of a chunk and commits them to the stage's mbarrier, which
+// the stagers wait on before overwriting the stage.  The accumulator (128
+// lanes x 128 FP32 columns of tensor memory) is read back by the four warps,
+// warp w holding rows 32w..32w+31.
+//
+// Few output tiles with a long K (the weight gradient: 256 x 256 over the
+// batch) split K across gridDim.z CTAs per tile; each writes its partial
+// tile to a workspace and k_sum_splits adds the splits in a fixed order, so
+// results do not depend on scheduling.  Every mbarrier wait gives up after
+// about a second, sets *err and skips the epilogue; tensor memory is freed
+// on every path.
+namespace tc {
+constexpr int BM = 128, BN = 128, BK = 64;
+constexpr u32 SBO_K = 128, LBO_K = 2048;         // K-major: row-group and k-group steps
+constexpr u32 SBO_MN = 144, LBO_MN = 2304;       // MN-major: row-group and k-group steps
+constexpr u32 CHUNK_BYTES = 8 * LBO_MN;          // one operand chunk (the larger layout)
+constexpr u32 STAGE_BYTES = 2 * CHUNK_BYTES;     // A chunk + B chunk
+constexpr u32 TMEM_COLS = 128;
+// Dynamic shared memory: two stages plus slack, so that any core matrix a
+// descriptor can name lies inside the allocation.
+constexpr u32 SMEM_BYTES = 2 * STAGE_BYTES + 48 * 1024;
+constexpr int MAX_SPLITS = 16;
 
-    for (int k0 = 0; k0 < K; k0 += 16) {
-        // stage A tile 64x16 and B tile 16x64 (8 elements per thread each)
-        for (int e = tid; e < 64 * 16; e += 128) {
-            int m = e / 16, k = e % 16;
-            sA[m][k] = TA ? A[(size_t)(k0 + k) * lda + (m0 + m)] : A[(size_t)(m0 + m) * lda + (k0 + k)];
-        }
-        for (int e = tid; e < 16 * 64; e += 128) {
-            int k = e / 64, nn = e % 64;
-            sB[k][nn] = TB ? B[(size_t)(n0 + nn) * ldb + (k0 + k)] : B[(size_t)(k0 + k) * ldb + (n0 + nn)];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int mi = 0; mi < 2; mi++) {
-            const int r = wm + mi * 16;
-            // A fragment (row-major 16x16): regs hold (row g | g+8, cols 2*t4 + {0,1} | +8)
-            u32 a0 = *reinterpret_cast<const u32 *>(&sA[r + g][2 * t4]);
-            u32 a1 = *reinterpret_cast<const u32 *>(&sA[r + g + 8][2 * t4]);
-            u32 a2 = *reinterpret_cast<const u32 *>(&sA[r + g][2 * t4 + 8]);
-            u32 a3 = *reinterpret_cast<const u32 *>(&sA[r + g + 8][2 * t4 + 8]);
-#pragma unroll
-            for (int ni = 0; ni < 4; ni++) {
-                const int c = wn + ni * 8;
-                // B fragment (16x8, k-major pairs): (k 2*t4 + {0,1} | +8, col g)
-                __nv_bfloat162 b01, b23;
-                b01.x = sB[2 * t4][c + g];
-                b01.y = sB[2 * t4 + 1][c + g];
-                b23.x = sB[2 * t4 + 8][c + g];
-                b23.y = sB[2 * t4 + 9][c + g];
-                u32 b0 = *reinterpret_cast<u32 *>(&b01), b1 = *reinterpret_cast<u32 *>(&b23);
-                asm volatile(
-                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-                    "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-                    : "+f"(acc[mi][ni][0]), "+f"(acc[mi][ni][1]), "+f"(acc[mi][ni][2]), "+f"(acc[mi][ni][3])
-                    : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-            }
-        }
-        __syncthreads();
+__device__ __forceinline__ u32 smem_addr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (no swizzle; version 1 at bit 46).
+__device__ __forceinline__ u64 smem_desc(u32 addr, u32 lbo, u32 sbo)
+{
+    return (u64)((addr & 0x3FFFFu) >> 4) | ((u64)(lbo >> 4) << 16) | ((u64)(sbo >> 4) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator (bit 4), BF16 A and B
+// (bits 7, 10), A / B MN-major (bits 15 / 16), N >> 3 at bit 17, M >> 4 at
+// bit 24.
+__host__ __device__ constexpr u32 instr_desc(int m, int n, bool a_mn, bool b_mn)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((u32)a_mn << 15) | ((u32)b_mn << 16) | ((u32)(n >> 3) << 17) |
+           ((u32)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(u32 bar, u32 parity)
+{
+    const long long t0 = clock64();
+    for (;;) {
+        u32 done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > 2000000000ll) return false;
     }
+}
+
+// Stages rows [row0, row0 + 128) x K [k0, k0 + 64) of an operand at `dst`.
+// KMAJOR: element (r, k) at src[r*ld + k], staged K-major; otherwise at
+// src[k*ld + r], staged MN-major.  Either way one 16-byte load and one
+// 16-byte store per 8 elements.
+template <bool KMAJOR>
+__device__ __forceinline__ void stage_chunk(uint8_t *dst, const __nv_bfloat16 *__restrict__ src, int ld, int row0,
+                                            int rows, int k0)
+{
+    const int tid = threadIdx.x;
+#pragma unroll 4
+    for (int v = tid; v < BM * BK / 8; v += 128) {
+        uint4 x = make_uint4(0, 0, 0, 0);
+        if (KMAJOR) {
+            // consecutive threads: consecutive rows of one 8-k group
+            const int kg = v >> 7, r = v & 127;
+            if (r < rows) x = *reinterpret_cast<const uint4 *>(src + (size_t)(row0 + r) * ld + k0 + kg * 8);
+            *reinterpret_cast<uint4 *>(dst + kg * LBO_K + (r >> 3) * SBO_K + (r & 7) * 16) = x;
+        } else {
+            // 16 consecutive threads: the 128 rows of one k
+            const int k = v >> 4, rg = v & 15;
+            if (rg * 8 < rows) x = *reinterpret_cast<const uint4 *>(src + (size_t)(k0 + k) * ld + row0 + rg * 8);
+            *reinterpret_cast<uint4 *>(dst + (k >> 3) * LBO_MN + rg * SBO_MN + (k & 7) * 16) = x;
+        }
+    }
+}
+}  // namespace tc
+
+// C (or, with gridDim.z > 1, split z's partial tile at C + z * split_stride)
+// for the tile (blockIdx.y, blockIdx.x) over this split's share of K.
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128, 1) k_gemm_tc(const __nv_bfloat16 *__restrict__ A, int lda,
+                                                     const __nv_bfloat16 *__restrict__ B, int ldb,
+                                                     float *__restrict__ C, int ldc, size_t split_stride, int M,
+                                                     int N, int K, u32 *__restrict__ err)
+{
+    using namespace tc;
+    constexpr bool A_KMAJOR = !TA, B_KMAJOR = TB;
+    constexpr u32 A_LBO = A_KMAJOR ? LBO_K : LBO_MN, A_SBO = A_KMAJOR ? SBO_K : SBO_MN;
+    constexpr u32 B_LBO = B_KMAJOR ? LBO_K : LBO_MN, B_SBO = B_KMAJOR ? SBO_K : SBO_MN;
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ u32 s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int rows_a = min(BM, M - m0), rows_b = min(BN, N - n0);
+    const int nk = K / BK, splits = gridDim.z, z = blockIdx.z;
+    const int kc0 = (int)((long long)z * nk / splits), kc1 = (int)((long long)(z + 1) * nk / splits);
+    const int cnt = kc1 - kc0;
+    C += (size_t)z * split_stride;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_addr(&s_tmem)), "r"(TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const u32 tmem = s_tmem;
+    const u32 idesc = instr_desc(BM, BN, !A_KMAJOR, !B_KMAJOR);
+
+    bool ok = true;
+    for (int j = 0; j < cnt && ok; j++) {
+        const int st = j & 1, kc = kc0 + j;
+        uint8_t *sa = smem + st * STAGE_BYTES, *sb = sa + CHUNK_BYTES;
+        // the MMAs of chunk j - 2 read this stage: wait for their commit
+        if (j >= 2) ok = mbar_wait(smem_addr(&bar[st]), ((j - 2) >> 1) & 1);
+        if (__syncthreads_and(ok) == 0) {
+            ok = false;
+            break;
+        }
+        stage_chunk<A_KMAJOR>(sa, A, lda, m0, rows_a, kc * BK);
+        stage_chunk<B_KMAJOR>(sb, B, ldb, n0, rows_b, kc * BK);
+        // generic-proxy stores -> visible to the tensor cores' async proxy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const u32 a0 = smem_addr(sa), b0 = smem_addr(sb);
 #pragma unroll
-    for (int mi = 0; mi < 2; mi++)
+            for (int kk = 0; kk < BK / 16; kk++) {
+                // one MMA consumes two 8-k groups
+                const u64 da = smem_desc(a0 + kk * 2 * A_LBO, A_LBO, A_SBO);
+                const u64 db = smem_desc(b0 + kk * 2 * B_LBO, B_LBO, B_SBO);
+                const u32 acc = (j > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{ .reg .pred p; setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p; }"
+                    :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u) : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(smem_addr(&bar[st])) : "memory");
+        }
+    }
+    // the last commit covers every MMA issued before it
+    if (ok && cnt > 0) ok = mbar_wait(smem_addr(&bar[(cnt - 1) & 1]), ((cnt - 1) >> 1) & 1);
+    ok = __syncthreads_and(ok) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok && cnt > 0) {
+        const int row = warp * 32 + lane;
+        float *out = C + (size_t)(m0 + row) * ldc + n0;
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 32) {
+            u32 v[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(tmem + ((u32)(warp * 32) << 16) + (u32)c));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < rows_a) {
 #pragma unroll
-        for (int ni = 0; ni < 4; ni++) {
-            int r = m0 + wm + mi * 16 + g, c = n0 + wn + ni * 8 + 2 * t4;
-            float *p0 = C + (size_t)r * ldc + c, *p1 = C + (size_t)(r + 8) * ldc + c;
-            if (beta != 0.f) {
-                p0[0] = beta * p0[0] + acc[mi][ni][0];
-                p0[1] = beta * p0[1] + acc[mi][ni][1];
-                p1[0] = beta * p1[0] + acc[mi][ni][2];
-                p1[1] = beta * p1[1] + acc[mi][ni][3];
-            } else {
-                p0[0] = acc[mi][ni][0];
-                p0[1] = acc[mi][ni][1];
-                p1[0] = acc[mi][ni][2];
-                p1[1] = acc[mi][ni][3];
+                for (int q = 0; q < 32; q += 4)
+                    *reinterpret_cast<float4 *>(out + c + q) =
+                        make_float4(__uint_as_float(v[q]), __uint_as_float(v[q + 1]), __uint_as_float(v[q + 2]),
+                                    __uint_as_float(v[q + 3]));
             }
         }
+    } else if (!ok && tid == 0) {
+        atomicOr(err, 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// C[m][n] (row stride ldc) = the sum over z = 0..splits-1, in that order, of
+// the partial tiles w[z][m][n] (M x N each).
+__global__ void k_sum_splits(const float *__restrict__ w, int splits, int M, int N, float *__restrict__ C, int ldc)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x, mn = (size_t)M * N;
+    if (i >= mn) return;
+    float acc = 0.f;
+    for (int z = 0; z < splits; z++) acc += w[z * mn + i];
+    C[(i / N) * ldc + i % N] = acc;
+}
+
+// K splits for a product: only when the output has under 32 tiles, about
+// four 64-wide K chunks per split, at most MAX_SPLITS, and only as many as
+// `work_elems` floats of workspace hold.
+inline int gemm_splits(int M, int N, int K, size_t work_elems)
+{
+    const int tiles = (N / tc::BN) * ((M + tc::BM - 1) / tc::BM), nk = K / tc::BK;
+    if (tiles >= 32) return 1;
+    int s = std::min(tc::MAX_SPLITS, std::max(1, nk / 4));
+    while (s > 1 && (size_t)s * M * N > work_elems) s--;
+    return s;
+}
+
+// Launches k_gemm_tc (see above for the operand layouts and size rules),
+// split over K into `work` (work_elems floats) when gemm_splits says so.
+template <bool TA, bool TB>
+inline cudaError_t gemm_tc(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int ldb, float *C, int ldc, int M,
+                           int N, int K, u32 *err, float *work, size_t work_elems, cudaStream_t s)
+{
+    if (M <= 0 || M % 8 || N <= 0 || N % tc::BN || K <= 0 || K % tc::BK) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tc::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    const int splits = work ? gemm_splits(M, N, K, work_elems) : 1;
+    dim3 grid(N / tc::BN, (M + tc::BM - 1) / tc::BM, splits);
+    if (splits == 1) {
+        k_gemm_tc<TA, TB><<<grid, 128, tc::SMEM_BYTES, s>>>(A, lda, B, ldb, C, ldc, 0, M, N, K, err);
+        return cudaGetLastError();
+    }
+    const size_t mn = (size_t)M * N;
+    k_gemm_tc<TA, TB><<<grid, 128, tc::SMEM_BYTES, s>>>(A, lda, B, ldb, work, N, mn, M, N, K, err);
+    k_sum_splits<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(work, splits, M, N, C, ldc);
+    return cudaGetLastError();
 }
 
 // h2 = relu(z2 + b2): FP32 and BF16 copies.

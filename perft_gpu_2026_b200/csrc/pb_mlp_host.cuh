@@ -36,13 +36,17 @@ struct Mlp {
     int16_t *idx = nullptr;
     float *h1f = nullptr, *z2 = nullptr, *h2f = nullptr, *y = nullptr, *dy = nullptr, *dh2f = nullptr,
           *dh1 = nullptr, *t = nullptr, *loss = nullptr;
+    u32 *err = nullptr;     // GEMM error word (a tensor-core wait that gave up)
+    float *work = nullptr;  // GEMM K-split partial tiles
+    static constexpr size_t WORK_ELEMS = (size_t)tc::MAX_SPLITS * MLP_H * MLP_H;
     __nv_bfloat16 *h1b = nullptr, *h2b = nullptr, *dh2b = nullptr;
     Board *pos_b = nullptr;
     uint8_t *pos_s = nullptr, *pos_c = nullptr;
 
     void release()
     {
-        void *ptrs[] = {p, g, m, v, pb, idx, h1f, z2, h2f, y, dy, dh2f, dh1, t, loss, h1b, h2b, dh2b, pos_b, pos_s, pos_c};
+        void *ptrs[] = {p,   g,   m,   v,   pb,  idx,  h1f,  z2,    h2f,   y,     dy,
+                        dh2f, dh1, t, loss, err, work, h1b, h2b, dh2b, pos_b, pos_s, pos_c};
         for (void *q : ptrs)
             if (q) cudaFree(q);
         *this = Mlp();
@@ -90,6 +94,9 @@ struct Mlp {
         if ((e = cudaMalloc(&v, bytes)) != cudaSuccess) return e;
         if ((e = cudaMalloc(&pb, MLP_PARAMS * sizeof(__nv_bfloat16))) != cudaSuccess) return e;
         if ((e = cudaMalloc(&loss, 64)) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&err, sizeof(u32))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&work, WORK_ELEMS * sizeof(float))) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(err, 0, sizeof(u32), s)) != cudaSuccess) return e;
         std::vector<float> h(MLP_PARAMS, 0.f);
         u64 st = seed;
         auto uni = [&](float lim) {
@@ -145,8 +152,9 @@ struct Mlp {
     {
         const __nv_bfloat16 *w1 = pb + MLP_OFF_W1, *w2 = pb + MLP_OFF_W2, *w3 = pb + MLP_OFF_W3;
         k_mlp_layer1<<<B, MLP_H, 0, s>>>(idx, w1, p + MLP_OFF_B1, B, h1f, h1b);
-        k_gemm_bf16<false, false><<<dim3(MLP_H / 64, B / 64), 128, 0, s>>>(h1b, MLP_H, w2, MLP_H, z2, MLP_H, B, MLP_H,
-                                                                         MLP_H, 0.f);
+        cudaError_t e =
+            gemm_tc<false, false>(h1b, MLP_H, w2, MLP_H, z2, MLP_H, B, MLP_H, MLP_H, err, work, WORK_ELEMS, s);
+        if (e != cudaSuccess) return e;
         size_t H = (size_t)B * MLP_H;
         k_bias_relu<<<(unsigned)((H + 255) / 256), 256, 0, s>>>(z2, p + MLP_OFF_B2, B, h2f, h2b);
         if (with_grad) cudaMemsetAsync(loss, 0, sizeof(float), s);
@@ -157,10 +165,12 @@ struct Mlp {
         k_back_h2<<<(unsigned)((H + 255) / 256), 256, 0, s>>>(dy, w3, h2f, B, dh2f, dh2b);
         k_colsum<<<1, MLP_H, 0, s>>>(dh2f, B, g + MLP_OFF_B2);
         // dW2 = h1^T dh2 ; dh1 = dh2 W2^T
-        k_gemm_bf16<true, false><<<dim3(MLP_H / 64, MLP_H / 64), 128, 0, s>>>(h1b, MLP_H, dh2b, MLP_H, g + MLP_OFF_W2,
-                                                                            MLP_H, MLP_H, MLP_H, B, 0.f);
-        k_gemm_bf16<false, true><<<dim3(MLP_H / 64, B / 64), 128, 0, s>>>(dh2b, MLP_H, w2, MLP_H, dh1, MLP_H, B,
-                                                                        MLP_H, MLP_H, 0.f);
+        if ((e = gemm_tc<true, false>(h1b, MLP_H, dh2b, MLP_H, g + MLP_OFF_W2, MLP_H, MLP_H, MLP_H, B, err, work,
+                                      WORK_ELEMS, s)) != cudaSuccess)
+            return e;
+        if ((e = gemm_tc<false, true>(dh2b, MLP_H, w2, MLP_H, dh1, MLP_H, B, MLP_H, MLP_H, err, work, WORK_ELEMS,
+                                      s)) != cudaSuccess)
+            return e;
         cudaMemsetAsync(g + MLP_OFF_W1, 0, sizeof(float) * ((size_t)MLP_IN * MLP_H + MLP_H), s);
         k_back_l1<<<B, MLP_H, 0, s>>>(idx, dh1, h1f, B, g + MLP_OFF_W1, g + MLP_OFF_B1);
         return cudaGetLastError();

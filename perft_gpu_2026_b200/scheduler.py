@@ -34,9 +34,9 @@ def label(eng: pg.Engine, positions, depths=(1, 2, 3, 4), chunk=262144):
     """Exact perft(k) for every position, as an (n, len(depths)) float64 array."""
     out = np.zeros((len(positions), len(depths)), dtype=np.float64)
     for c0 in range(0, len(positions), chunk):
-        part = positions[c0:c0 + chunk]
+        part = pg.pack_positions(positions[c0:c0 + chunk])
         for j, d in enumerate(depths):
-            out[c0:c0 + len(part), j] = eng.perft_batch(part, [d] * len(part))
+            out[c0:c0 + len(part), j] = eng.perft_batch(part, d)
     return out
 
 

@@ -5,6 +5,7 @@ that produced them.
     python profile_workloads.py leaf   [--depth 7] [--arena-gb 2] [--reps 3] [--leaf-kernel K] [--leaf-threads T]
     python profile_workloads.py levels [--roots 16384] [--depth 5] [--arena-gb 6]
     python profile_workloads.py tt     [--depth 8] [--dtt-mb 2000] [--arena-gb 2]
+    python profile_workloads.py gemm   [--m 4096] [--n 256] [--k 256] [--ta 0] [--tb 0] [--reps 20]
 
 leaf    the bench position (4 random plies from the initial array, splitmix64
         seed 1) at perft --depth without tables, --reps times: each pass is
@@ -18,6 +19,12 @@ levels  one batched perft over --roots playout positions (0..60 plies, seed
 tt      the start position with device tables: perft depth-1 (fills the
         tables), then perft depth (the launch to capture: skip the first
         table-leaf launch).  Counts are checked against the known totals.
+gemm    the scheduler network's tcgen05 GEMM on random BF16 operands: one
+        checked launch, then --reps timed launches (CUDA events); prints the
+        mean time and TFLOP/s.  The network's three products at a 4096-sample
+        batch are (--ta 0 --tb 0 --m 4096 --n 256 --k 256: layer 2 forward),
+        (--ta 1 --m 256 --k 4096: its weight gradient) and (--tb 1 --m 4096:
+        its input gradient).
 """
 from __future__ import annotations
 
@@ -82,6 +89,26 @@ def tt(args):
     eng.close()
 
 
+def gemm(args):
+    import numpy as np
+
+    rng = np.random.default_rng(1)
+    m, n, k = args.m, args.n, args.k
+    a = rng.uniform(-1, 1, size=m * k).astype(np.float32)
+    b = rng.uniform(-1, 1, size=k * n).astype(np.float32)
+    to_bits = lambda x: ((x.view(np.uint32) + 0x8000) >> 16).astype(np.uint16)
+    eng = pg.Engine(device=0, use_tt=False, arena_bytes=1 << 28)
+    c, ms = eng.selftest_gemm(to_bits(a), to_bits(b), bool(args.ta), bool(args.tb), m, n, k, reps=args.reps)
+    av = (to_bits(a).astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+    bv = (to_bits(b).astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+    am = av.reshape(k, m).T if args.ta else av.reshape(m, k)
+    bm = bv.reshape(n, k).T if args.tb else bv.reshape(k, n)
+    err = float(np.abs(c - am @ bm).max())
+    print(json.dumps({"workload": "gemm", "m": m, "n": n, "k": k, "ta": args.ta, "tb": args.tb, "reps": args.reps,
+                      "ms": ms, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12, "max_abs_err": err}))
+    eng.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="which", required=True)
@@ -100,8 +127,15 @@ def main(argv=None):
     a.add_argument("--depth", type=int, default=8)
     a.add_argument("--dtt-mb", type=int, default=2000)
     a.add_argument("--arena-gb", type=int, default=2)
+    a = sub.add_parser("gemm")
+    a.add_argument("--m", type=int, default=4096)
+    a.add_argument("--n", type=int, default=256)
+    a.add_argument("--k", type=int, default=256)
+    a.add_argument("--ta", type=int, default=0)
+    a.add_argument("--tb", type=int, default=0)
+    a.add_argument("--reps", type=int, default=20)
     args = ap.parse_args(argv)
-    {"leaf": leaf, "levels": levels, "tt": tt}[args.which](args)
+    {"leaf": leaf, "levels": levels, "tt": tt, "gemm": gemm}[args.which](args)
     return 0
 
 

@@ -1,6 +1,6 @@
 """The scheduler network's hand-written kernels (embedding-bag layer 1, BF16
-tensor-core GEMMs, Adam) against the FP32 numpy restatement: forward values,
-loss and every parameter gradient."""
+tcgen05 tensor-core GEMMs, Adam) against the FP32 numpy restatement: the GEMM
+alone, forward values, loss and every parameter gradient."""
 import numpy as np
 import pytest
 
@@ -23,6 +23,35 @@ def _batch(n, seed):
     rng = np.random.default_rng(seed)
     t = rng.uniform(0, 20, size=(n, 4)).astype(np.float32)
     return pos, t
+
+
+def _bf16(x):
+    """float32 -> (BF16 bit patterns, the float32 values they hold); round to nearest even."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32)
+    bits = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+    return bits, (bits.astype(np.uint32) << 16).view(np.float32)
+
+
+@pytest.mark.parametrize("ta,tb,m,n,k", [(0, 0, 192, 256, 256), (1, 0, 256, 256, 448), (0, 1, 200, 256, 256),
+                                         (1, 1, 8, 128, 64), (0, 0, 4096, 256, 256), (1, 0, 256, 256, 4096),
+                                         (1, 0, 136, 256, 1088), (0, 0, 128, 128, 640)])
+def test_tensor_core_gemm_matches_numpy(eng, ta, tb, m, n, k):
+    """k_gemm_tc against a float64 product of the same BF16 values: partial
+    row tiles (M = 192, 200, 136, 8), an odd number of K chunks (448 = 7 x
+    64), K split over CTAs (the weight-gradient shape 256 x 256 x 4096: 16
+    splits of 4 chunks; 1088 = 17 chunks in 4 uneven splits; 640 = 10 chunks
+    in 2), every transpose combination the network uses and one it does not."""
+    rng = np.random.default_rng(m * 7 + k + 3 * ta + tb)
+    a = rng.uniform(-1, 1, size=(m, k)).astype(np.float32)
+    b = rng.uniform(-1, 1, size=(k, n)).astype(np.float32)
+    a_bits, a_val = _bf16(a.T.copy() if ta else a)
+    b_bits, b_val = _bf16(b.T.copy() if tb else b)
+    a_ref = (a_val.T if ta else a_val).astype(np.float64)
+    b_ref = (b_val.T if tb else b_val).astype(np.float64)
+    c = eng.selftest_gemm(a_bits, b_bits, bool(ta), bool(tb), m, n, k)
+    want = a_ref @ b_ref
+    # exact BF16 products, FP32 accumulation over k terms
+    assert np.abs(c - want).max() <= 1e-5 * k + 1e-4, np.abs(c - want).max()
 
 
 def test_gradients_match_numpy_reference(eng):

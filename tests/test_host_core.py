@@ -102,6 +102,27 @@ def test_uneven_roots_have_moves():
     assert [r.key() for r in roots] == [r.key() for r in again]
 
 
+def test_packed_positions_and_per_root_ints():
+    """The batch format of the C ABI: packing a list copies the positions in
+    order, a packed array passes through as the same object, and per-root
+    ints accept one int for all or one per root (the wrong length is refused)."""
+    roots = pg.random_playouts(5, 64, 0, 30)
+    packed = pg.random_playouts(5, 64, 0, 30, packed=True)
+    assert isinstance(packed, ctypes.Array) and len(packed) == 64
+    assert [p.key() for p in packed] == [p.key() for p in roots]
+    again = pg.pack_positions(roots)
+    assert [p.key() for p in again] == [p.key() for p in roots]
+    assert pg.pack_positions(packed) is packed
+    assert pg._c_ints(5, 3).tolist() == [5, 5, 5]
+    assert pg._c_ints([1, 2, 3], 3).tolist() == [1, 2, 3]
+    with pytest.raises(ValueError):
+        pg._c_ints([1, 2], 3)
+    # a batch call without a GPU reaches the library with the packed arrays
+    eng = pg.Engine(device=-1)
+    with pytest.raises(pg.PerftError):
+        eng.perft_batch(packed, 3)
+
+
 def test_cpu_cli_output_format():
     import os
     import subprocess
