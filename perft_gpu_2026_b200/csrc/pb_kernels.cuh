@@ -998,6 +998,14 @@ __device__ __forceinline__ u64 dev_size(const u64 *n_dev, u64 cap, u32 *err)
     return n;
 }
 
+// True in every thread of the CTA when a level already outgrew its plan: the
+// batch will be rerun, so its leaf leaves at once instead of counting
+// truncated levels.  Called by all threads before any other barrier.
+__device__ __forceinline__ bool plan_overflowed(const u32 *err)
+{
+    return __syncthreads_or((*reinterpret_cast<const volatile u32 *>(err) & DEVERR_OVERFLOW) != 0) != 0;
+}
+
 // The same leaf with the level sizes in device memory, for captured graphs:
 // the grid covers the planned capacity and the CTAs past the level's actual
 // size leave at once (a whole CTA at a time, so the ranking's barriers are
@@ -1010,6 +1018,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
                        const u64 *__restrict__ npar_dev, u64 npar_cap, unsigned long long *__restrict__ root_counts,
                        unsigned long long *__restrict__ counter, u32 *__restrict__ err)
 {
+    if (plan_overflowed(err)) return;
     const u64 n = dev_size(n_dev, cap, err);
     if ((u64)blockIdx.x * blockDim.x >= n) return;
     const u64 npar = min(*npar_dev, npar_cap);
@@ -1028,6 +1037,7 @@ __global__ void __launch_bounds__(T, 1024 / T)
                                 unsigned long long *__restrict__ root_counts, unsigned long long *__restrict__ counter,
                                 u32 *__restrict__ err)
 {
+    if (plan_overflowed(err)) return;
     const u64 n = dev_size(n_dev, cap, err);
     if ((u64)blockIdx.x * (PB_BALANCED_K * T) >= n) return;
     const u64 npar = min(*npar_dev, npar_cap);
@@ -1155,6 +1165,7 @@ __global__ void __launch_bounds__(PB_LEAF_THREADS, PB_LEAF_MIN_BLOCKS)
                          unsigned long long *__restrict__ root_counts, unsigned long long *__restrict__ counter,
                          u32 *__restrict__ err)
 {
+    if (plan_overflowed(err)) return;
     const u64 n = dev_size(n_dev, cap, err);
     const u64 npar = min(*npar_dev, npar_cap);
     const int lane = threadIdx.x & 31;
