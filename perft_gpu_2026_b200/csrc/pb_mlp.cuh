@@ -12,6 +12,7 @@
 // operands, FP32 accumulation in tensor memory); layer 3 (256x4) is a
 // per-sample dot product.
 #pragma once
+#include <cuda.h>  // CUtensorMap; the encoder is taken from the driver at run time
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -75,27 +76,30 @@ __global__ void k_mlp_layer1(const int16_t *__restrict__ idx, const __nv_bfloat1
 
 // ---------------------------------------------------------------- tensor-core GEMM
 // C[M x N] (FP32) = A[M x K] * B[K x N], BF16 operands, FP32 accumulation in
-// tensor memory, on the 5th-generation tensor cores (tcgen05).
+// tensor memory, on the 5th-generation tensor cores (tcgen05), operands
+// brought into shared memory by the tensor memory accelerator (TMA).
 //
 // Element (m, k) of A is A[m*lda + k], or with TA A[k*lda + m]; element
 // (k, n) of B is B[k*ldb + n], or with TB B[n*ldb + k].  M a multiple of 8
-// (rows past M read as zero and are not stored), N of 128, K of 64.
+// (rows past M read as zero and are not stored), N of 128, K of 64; base
+// addresses 16-byte aligned, lda and ldb multiples of 8.
 //
 // One CTA of 128 threads per 128 x 128 tile of C (and per K split, below).
-// K advances 64 at a time through two shared-memory stages: all threads
-// stage the next A and B chunks with 16-byte loads and stores while the
-// tensor cores work on the current one.  Each operand keeps the layout it
-// has in global memory, in one of the two canonical no-swizzle layouts of
-// 8 x 16-byte core matrices: K-major (an operand contiguous along K: a
-// core matrix is 8 rows x 8 k; 8-row groups SBO_K = 128 B apart, 8-k groups
-// LBO_K = 2048 B apart) or MN-major (contiguous along M or N: a core matrix
-// is 8 k x 8 rows; 8-row groups SBO_MN = 144 B apart, so that 16 threads
-// storing one k row hit distinct banks, and 8-k groups LBO_MN = 2304 B
-// apart); the instruction descriptor names which.  Thread 0 issues the four
-// 128x128x16 MMAs of a chunk and commits them to the stage's mbarrier, which
-// the stagers wait on before overwriting the stage.  The accumulator (128
-// lanes x 128 FP32 columns of tensor memory) is read back by the four warps,
-// warp w holding rows 32w..32w+31.
+// K advances 64 at a time through a ring of four shared-memory stages.
+// Thread 0 keeps up to four chunks of both operands in flight with
+// cp.async.bulk.tensor loads (each stage's mbarrier counts the bytes in),
+// issues the four 128x128x16 tcgen05.mma of a chunk once its bytes have
+// landed, and commits them to the stage's second mbarrier, which it waits on
+// before loading the stage again.  Each operand keeps the layout it has in
+// global memory, as one of the two canonical 128-byte-swizzled layouts that
+// TMA writes and the MMA reads: K-major for an operand contiguous along K
+// (one 64 x 128 box: rows of 64 k, 8-row groups 1024 B apart; an MMA's
+// 16-k step moves the start address 32 B) or MN-major for one contiguous
+// along M or N (two 64 x 64 boxes of 64 k rows x 64 elements: 8-k groups
+// 1024 B apart, the two 64-wide halves 8192 B apart; a 16-k step moves
+// 2048 B); the instruction descriptor names which.  A last commit to a
+// third mbarrier tells all four warps the accumulator (128 lanes x 128 FP32
+// columns of tensor memory) is final; warp w reads rows 32w..32w+31 back.
 //
 // Few output tiles with a long K (the weight gradient: 256 x 256 over the
 // batch) split K across gridDim.z CTAs per tile; each writes its partial
@@ -104,23 +108,21 @@ __global__ void k_mlp_layer1(const int16_t *__restrict__ idx, const __nv_bfloat1
 // about a second, sets *err and skips the epilogue; tensor memory is freed
 // on every path.
 namespace tc {
-constexpr int BM = 128, BN = 128, BK = 64;
-constexpr u32 SBO_K = 128, LBO_K = 2048;         // K-major: row-group and k-group steps
-constexpr u32 SBO_MN = 144, LBO_MN = 2304;       // MN-major: row-group and k-group steps
-constexpr u32 CHUNK_BYTES = 8 * LBO_MN;          // one operand chunk (the larger layout)
-constexpr u32 STAGE_BYTES = 2 * CHUNK_BYTES;     // A chunk + B chunk
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4;
+constexpr u32 OPERAND_BYTES = BM * BK * 2;         // one operand chunk, 16 KB
+constexpr u32 STAGE_BYTES = 2 * OPERAND_BYTES;     // A chunk + B chunk
+constexpr u32 SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + slack to align the ring to 1024 B
 constexpr u32 TMEM_COLS = 128;
-// Dynamic shared memory: two stages plus slack, so that any core matrix a
-// descriptor can name lies inside the allocation.
-constexpr u32 SMEM_BYTES = 2 * STAGE_BYTES + 48 * 1024;
 constexpr int MAX_SPLITS = 16;
 
 __device__ __forceinline__ u32 smem_addr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
 
-// Shared-memory matrix descriptor (no swizzle; version 1 at bit 46).
-__device__ __forceinline__ u64 smem_desc(u32 addr, u32 lbo, u32 sbo)
+// Shared-memory matrix descriptor, 128-byte swizzle (layout type 2 at bit
+// 61), version 1 at bit 46.
+__device__ __forceinline__ u64 smem_desc_sw128(u32 addr, u32 lbo, u32 sbo)
 {
-    return (u64)((addr & 0x3FFFFu) >> 4) | ((u64)(lbo >> 4) << 16) | ((u64)(sbo >> 4) << 32) | (1ull << 46);
+    return (u64)((addr & 0x3FFFFu) >> 4) | ((u64)(lbo >> 4) << 16) | ((u64)(sbo >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
 }
 
 // Instruction descriptor, kind::f16: FP32 accumulator (bit 4), BF16 A and B
@@ -147,55 +149,59 @@ __device__ __forceinline__ bool mbar_wait(u32 bar, u32 parity)
     }
 }
 
-// Stages rows [row0, row0 + 128) x K [k0, k0 + 64) of an operand at `dst`.
-// KMAJOR: element (r, k) at src[r*ld + k], staged K-major; otherwise at
-// src[k*ld + r], staged MN-major.  Either way one 16-byte load and one
-// 16-byte store per 8 elements.
-template <bool KMAJOR>
-__device__ __forceinline__ void stage_chunk(uint8_t *dst, const __nv_bfloat16 *__restrict__ src, int ld, int row0,
-                                            int rows, int k0)
+// A 2-D TMA tile load of this CTA's own box into shared memory at `dst`, counted
+// into mbarrier `bar`; x (the contiguous coordinate) a multiple of 64.
+__device__ __forceinline__ void tma_load_2d(u32 dst, const CUtensorMap *map, int x, int y, u32 bar)
 {
-    const int tid = threadIdx.x;
-#pragma unroll 4
-    for (int v = tid; v < BM * BK / 8; v += 128) {
-        uint4 x = make_uint4(0, 0, 0, 0);
-        if (KMAJOR) {
-            // consecutive threads: consecutive rows of one 8-k group
-            const int kg = v >> 7, r = v & 127;
-            if (r < rows) x = *reinterpret_cast<const uint4 *>(src + (size_t)(row0 + r) * ld + k0 + kg * 8);
-            *reinterpret_cast<uint4 *>(dst + kg * LBO_K + (r >> 3) * SBO_K + (r & 7) * 16) = x;
-        } else {
-            // 16 consecutive threads: the 128 rows of one k
-            const int k = v >> 4, rg = v & 15;
-            if (rg * 8 < rows) x = *reinterpret_cast<const uint4 *>(src + (size_t)(k0 + k) * ld + row0 + rg * 8);
-            *reinterpret_cast<uint4 *>(dst + (k >> 3) * LBO_MN + rg * SBO_MN + (k & 7) * 16) = x;
-        }
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        :: "r"(dst), "l"(reinterpret_cast<u64>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// One operand chunk (64 k x 128 rows from row0, k from k0) into stage memory
+// at `dst`.
+template <bool KMAJOR>
+__device__ __forceinline__ void load_operand(u32 dst, const CUtensorMap *map, int row0, int k0, u32 bar)
+{
+    if (KMAJOR) {
+        tma_load_2d(dst, map, k0, row0, bar);
+    } else {
+        tma_load_2d(dst, map, row0, k0, bar);
+        tma_load_2d(dst + OPERAND_BYTES / 2, map, row0 + 64, k0, bar);
     }
+}
+
+// Descriptor of the 16-k slice kk (0..3) of an operand chunk at `base`.
+template <bool KMAJOR>
+__device__ __forceinline__ u64 operand_desc(u32 base, int kk)
+{
+    return KMAJOR ? smem_desc_sw128(base + kk * 32, 16, 1024) : smem_desc_sw128(base + kk * 2048, 8192, 1024);
 }
 }  // namespace tc
 
 // C (or, with gridDim.z > 1, split z's partial tile at C + z * split_stride)
 // for the tile (blockIdx.y, blockIdx.x) over this split's share of K.
 template <bool TA, bool TB>
-__global__ void __launch_bounds__(128, 1) k_gemm_tc(const __nv_bfloat16 *__restrict__ A, int lda,
-                                                     const __nv_bfloat16 *__restrict__ B, int ldb,
+__global__ void __launch_bounds__(128, 1) k_gemm_tc(const __grid_constant__ CUtensorMap map_a,
+                                                     const __grid_constant__ CUtensorMap map_b,
                                                      float *__restrict__ C, int ldc, size_t split_stride, int M,
                                                      int N, int K, u32 *__restrict__ err)
 {
     using namespace tc;
     constexpr bool A_KMAJOR = !TA, B_KMAJOR = TB;
-    constexpr u32 A_LBO = A_KMAJOR ? LBO_K : LBO_MN, A_SBO = A_KMAJOR ? SBO_K : SBO_MN;
-    constexpr u32 B_LBO = B_KMAJOR ? LBO_K : LBO_MN, B_SBO = B_KMAJOR ? SBO_K : SBO_MN;
-    extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bar[2];
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
     __shared__ u32 s_tmem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const int rows_a = min(BM, M - m0), rows_b = min(BN, N - n0);
+    const int rows_a = min(BM, M - m0);
     const int nk = K / BK, splits = gridDim.z, z = blockIdx.z;
     const int kc0 = (int)((long long)z * nk / splits), kc1 = (int)((long long)(z + 1) * nk / splits);
     const int cnt = kc1 - kc0;
     C += (size_t)z * split_stride;
+    // the stage ring, aligned to the 1024-byte swizzle atom
+    const u32 ring = (smem_addr(smem) + 1023u) & ~1023u;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -203,39 +209,44 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const __nv_bfloat16 *__restr
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&bar[1])) : "memory");
+        for (int st = 0; st < STAGES; st++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&full[st])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&empty[st])) : "memory");
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&done)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" :: "l"(reinterpret_cast<u64>(&map_a)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" :: "l"(reinterpret_cast<u64>(&map_b)) : "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const u32 tmem = s_tmem;
-    const u32 idesc = instr_desc(BM, BN, !A_KMAJOR, !B_KMAJOR);
 
     bool ok = true;
-    for (int j = 0; j < cnt && ok; j++) {
-        const int st = j & 1, kc = kc0 + j;
-        uint8_t *sa = smem + st * STAGE_BYTES, *sb = sa + CHUNK_BYTES;
-        // the MMAs of chunk j - 2 read this stage: wait for their commit
-        if (j >= 2) ok = mbar_wait(smem_addr(&bar[st]), ((j - 2) >> 1) & 1);
-        if (__syncthreads_and(ok) == 0) {
-            ok = false;
-            break;
-        }
-        stage_chunk<A_KMAJOR>(sa, A, lda, m0, rows_a, kc * BK);
-        stage_chunk<B_KMAJOR>(sb, B, ldb, n0, rows_b, kc * BK);
-        // generic-proxy stores -> visible to the tensor cores' async proxy
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+    if (tid == 0 && cnt > 0) {
+        const u32 idesc = instr_desc(BM, BN, !A_KMAJOR, !B_KMAJOR);
+        auto issue = [&](int j) {
+            const int st = j % STAGES;
+            const u32 a = ring + st * STAGE_BYTES, b = a + OPERAND_BYTES, bar = smem_addr(&full[st]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(STAGE_BYTES)
+                         : "memory");
+            load_operand<A_KMAJOR>(a, &map_a, m0, (kc0 + j) * BK, bar);
+            load_operand<B_KMAJOR>(b, &map_b, n0, (kc0 + j) * BK, bar);
+        };
+        for (int j = 0; j < cnt && j < STAGES; j++) issue(j);
+        for (int j = 0; j < cnt; j++) {
+            const int st = j % STAGES;
+            const u32 ph = (u32)(j / STAGES) & 1u;
+            if (!mbar_wait(smem_addr(&full[st]), ph)) {
+                ok = false;
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const u32 a0 = smem_addr(sa), b0 = smem_addr(sb);
+            const u32 a = ring + st * STAGE_BYTES, b = a + OPERAND_BYTES;
 #pragma unroll
             for (int kk = 0; kk < BK / 16; kk++) {
-                // one MMA consumes two 8-k groups
-                const u64 da = smem_desc(a0 + kk * 2 * A_LBO, A_LBO, A_SBO);
-                const u64 db = smem_desc(b0 + kk * 2 * B_LBO, B_LBO, B_SBO);
+                const u64 da = operand_desc<A_KMAJOR>(a, kk), db = operand_desc<B_KMAJOR>(b, kk);
                 const u32 acc = (j > 0 || kk > 0) ? 1u : 0u;
                 asm volatile(
                     "{ .reg .pred p; setp.ne.b32 p, %4, 0;\n\t"
@@ -243,11 +254,22 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const __nv_bfloat16 *__restr
                     :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u) : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         :: "r"(smem_addr(&bar[st])) : "memory");
+                         :: "r"(smem_addr(&empty[st])) : "memory");
+            if (j + STAGES < cnt) {
+                // the stage is free once this chunk's MMAs have read it
+                if (!mbar_wait(smem_addr(&empty[st]), ph)) {
+                    ok = false;
+                    break;
+                }
+                issue(j + STAGES);
+            }
         }
+        // covers every MMA issued before it
+        if (ok)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(smem_addr(&done)) : "memory");
     }
-    // the last commit covers every MMA issued before it
-    if (ok && cnt > 0) ok = mbar_wait(smem_addr(&bar[(cnt - 1) & 1]), ((cnt - 1) >> 1) & 1);
+    if (cnt > 0 && __syncthreads_and(ok)) ok = mbar_wait(smem_addr(&done), 0);
     ok = __syncthreads_and(ok) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok && cnt > 0) {
@@ -309,24 +331,76 @@ inline int gemm_splits(int M, int N, int K, size_t work_elems)
     return s;
 }
 
+// The driver's tensor-map encoder, looked up once through the runtime (the
+// library does not link the driver library itself).
+typedef CUresult (*TensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                         const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                         CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                         CUtensorMapFloatOOBfill);
+inline TensorMapEncodeTiled tensor_map_encoder()
+{
+    static TensorMapEncodeTiled fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<TensorMapEncodeTiled>(f);
+    }();
+    return fn;
+}
+
+// Tensor map of a row-major BF16 matrix (`outer` rows of `inner` elements,
+// `ld` elements apart) read in boxes of box_inner x box_outer with the
+// 128-byte swizzle; boxes reaching past the matrix read zeros.
+inline cudaError_t make_tensor_map(CUtensorMap *map, const __nv_bfloat16 *base, u64 inner, u64 outer, u64 ld,
+                                   u32 box_inner, u32 box_outer)
+{
+    TensorMapEncodeTiled encode = tensor_map_encoder();
+    if (!encode) return cudaErrorNotSupported;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld * 2) % 16) return cudaErrorInvalidValue;
+    const cuuint64_t dims[2] = {inner, outer};
+    const cuuint64_t strides[1] = {ld * 2};
+    const cuuint32_t box[2] = {box_inner, box_outer};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(base), dims, strides,
+                        box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// Tensor map of one GEMM operand: `rows` (M or N) x K, K-major when the
+// operand is contiguous along K (element (r, k) at p[r*ld + k]: boxes of 64 k
+// x 128 rows), MN-major otherwise (element (r, k) at p[k*ld + r]: boxes of
+// 64 rows x 64 k).
+inline cudaError_t operand_map(CUtensorMap *map, const __nv_bfloat16 *p, bool kmajor, int rows, int K, int ld)
+{
+    return kmajor ? make_tensor_map(map, p, (u64)K, (u64)rows, (u64)ld, tc::BK, tc::BM)
+                  : make_tensor_map(map, p, (u64)rows, (u64)K, (u64)ld, 64, tc::BK);
+}
+
 // Launches k_gemm_tc (see above for the operand layouts and size rules),
 // split over K into `work` (work_elems floats) when gemm_splits says so.
 template <bool TA, bool TB>
 inline cudaError_t gemm_tc(const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *B, int ldb, float *C, int ldc, int M,
                            int N, int K, u32 *err, float *work, size_t work_elems, cudaStream_t s)
 {
-    if (M <= 0 || M % 8 || N <= 0 || N % tc::BN || K <= 0 || K % tc::BK) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)tc::SMEM_BYTES);
+    if (M <= 0 || M % 8 || N <= 0 || N % tc::BN || K <= 0 || K % tc::BK || lda % 8 || ldb % 8)
+        return cudaErrorInvalidValue;
+    CUtensorMap map_a, map_b;
+    cudaError_t e = operand_map(&map_a, A, !TA, M, K, lda);
+    if (e == cudaSuccess) e = operand_map(&map_b, B, TB, N, K, ldb);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES);
     if (e != cudaSuccess) return e;
     const int splits = work ? gemm_splits(M, N, K, work_elems) : 1;
     dim3 grid(N / tc::BN, (M + tc::BM - 1) / tc::BM, splits);
     if (splits == 1) {
-        k_gemm_tc<TA, TB><<<grid, 128, tc::SMEM_BYTES, s>>>(A, lda, B, ldb, C, ldc, 0, M, N, K, err);
+        k_gemm_tc<TA, TB><<<grid, 128, tc::SMEM_BYTES, s>>>(map_a, map_b, C, ldc, 0, M, N, K, err);
         return cudaGetLastError();
     }
     const size_t mn = (size_t)M * N;
-    k_gemm_tc<TA, TB><<<grid, 128, tc::SMEM_BYTES, s>>>(A, lda, B, ldb, work, N, mn, M, N, K, err);
+    k_gemm_tc<TA, TB><<<grid, 128, tc::SMEM_BYTES, s>>>(map_a, map_b, work, N, mn, M, N, K, err);
     k_sum_splits<<<(unsigned)((mn + 255) / 256), 256, 0, s>>>(work, splits, M, N, C, ldc);
     return cudaGetLastError();
 }
