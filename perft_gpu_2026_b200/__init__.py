@@ -311,6 +311,15 @@ def pack_positions(roots) -> ctypes.Array:
     return (Pos * len(roots))(*roots)
 
 
+def pack_slice(roots, a: int, b: int) -> ctypes.Array:
+    """Positions a..b-1 as a packed array: a view sharing the memory of a
+    packed array (no copy), or a copy of that part of a sequence of Pos."""
+    if isinstance(roots, ctypes.Array) and roots._type_ is Pos:
+        b = min(b, len(roots))
+        return (Pos * max(b - a, 0)).from_buffer(roots, a * ctypes.sizeof(Pos))
+    return pack_positions(roots[a:b])
+
+
 def _c_ints(values, n: int):
     """Per-position ints (or one int for all) as a contiguous C int array."""
     import numpy as np

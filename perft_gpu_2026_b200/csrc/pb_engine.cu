@@ -2550,36 +2550,49 @@ int pb_mlp_train(pb_ctx *ctx, const pb_pos *pos, const float *targets, int n, in
     Mlp &m = ctx->mlp;
     cudaStream_t s = ctx->stream;
     PB_CUDA(m.alloc_batch(batch));
+    // The training set goes to the device once (feature indices and
+    // targets); every step gathers its batch there, so a step is kernel
+    // launches only and the host reads the loss once per epoch.
+    DeviceBuffer<int16_t> all_idx;
+    DeviceBuffer<float> all_t;
+    DeviceBuffer<int> order_d;
+    DeviceBuffer<double> acc;
+    PB_CUDA(all_idx.alloc((size_t)n * MLP_MAX_ACTIVE));
+    PB_CUDA(all_t.alloc((size_t)n * MLP_OUT));
+    PB_CUDA(order_d.alloc((size_t)n));
+    PB_CUDA(acc.alloc(1));
+    for (int c0 = 0; c0 < n; c0 += batch) {
+        const int k = std::min(batch, n - c0);
+        PB_CUDA(m.features_to(pos + c0, k, all_idx.p + (size_t)c0 * MLP_MAX_ACTIVE, s));
+    }
+    PB_CUDA(cudaMemcpyAsync(all_t.p, targets, sizeof(float) * MLP_OUT * (size_t)n, cudaMemcpyHostToDevice, s));
     std::vector<int> order(n);
     for (int i = 0; i < n; i++) order[i] = i;
-    std::vector<pb_pos> bp(batch);
-    std::vector<float> bt((size_t)batch * MLP_OUT);
     u64 rng = seed;
     double epoch_loss = 0;
+    const int V = MLP_MAX_ACTIVE * (int)sizeof(int16_t) / 16 + 1;  // gather threads per row
     for (int ep = 0; ep < epochs; ep++) {
         for (int i = n - 1; i > 0; i--) {
             u64 r = splitmix64(&rng);
             int j = (int)(((unsigned __int128)r * (u64)(i + 1)) >> 64);
             std::swap(order[i], order[j]);
         }
-        epoch_loss = 0;
+        PB_CUDA(cudaMemcpyAsync(order_d.p, order.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+        PB_CUDA(cudaMemsetAsync(acc.p, 0, sizeof(double), s));
         int steps = 0;
         for (int b0 = 0; b0 + batch <= n; b0 += batch) {
-            for (int k = 0; k < batch; k++) {
-                bp[k] = pos[order[b0 + k]];
-                memcpy(&bt[(size_t)k * MLP_OUT], targets + (size_t)order[b0 + k] * MLP_OUT, sizeof(float) * MLP_OUT);
-            }
-            PB_CUDA(m.load_positions(bp.data(), batch, s));
-            PB_CUDA(cudaMemcpyAsync(m.t, bt.data(), sizeof(float) * bt.size(), cudaMemcpyHostToDevice, s));
+            k_gather_batch<<<(batch * V + 255) / 256, 256, 0, s>>>(all_idx.p, all_t.p, order_d.p, b0, batch, m.idx,
+                                                                  m.t);
             PB_CUDA(m.forward_backward(batch, true, s));
             PB_CUDA(m.adam_step(lr, s));
-            float l = 0;
-            PB_CUDA(cudaMemcpyAsync(&l, m.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
-            PB_CUDA(cudaStreamSynchronize(s));
-            epoch_loss += l / (double)(batch * MLP_OUT);
+            k_accum_loss<<<1, 32, 0, s>>>(m.loss, acc.p, 1.0 / (double)(batch * MLP_OUT));
             steps++;
         }
-        if (steps) epoch_loss /= steps;
+        PB_CUDA(cudaGetLastError());
+        double total = 0;
+        PB_CUDA(cudaMemcpyAsync(&total, acc.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+        epoch_loss = steps ? total / steps : 0.0;
     }
     if (final_loss) *final_loss = (float)epoch_loss;
     return mlp_check(ctx);

@@ -52,6 +52,32 @@ __global__ void k_features(const Board *__restrict__ boards, const uint8_t *__re
     while (k < MLP_MAX_ACTIVE) o[k++] = -1;
 }
 
+// Training batch from the device-resident training set: row k of the batch
+// is example order[b0 + k] (feature indices, 80 B, and targets, 16 B, as
+// 16-byte vectors).
+__global__ void k_gather_batch(const int16_t *__restrict__ all_idx, const float *__restrict__ all_t,
+                               const int *__restrict__ order, int b0, int B, int16_t *__restrict__ idx,
+                               float *__restrict__ t)
+{
+    static_assert(MLP_MAX_ACTIVE * sizeof(int16_t) % 16 == 0 && MLP_OUT * sizeof(float) == 16, "16-byte rows");
+    constexpr int V = MLP_MAX_ACTIVE * (int)sizeof(int16_t) / 16;  // vectors per feature row
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B * (V + 1)) return;
+    const int k = i / (V + 1), v = i % (V + 1);
+    const size_t src = (size_t)order[b0 + k];
+    if (v < V)
+        reinterpret_cast<uint4 *>(idx + (size_t)k * MLP_MAX_ACTIVE)[v] =
+            reinterpret_cast<const uint4 *>(all_idx + src * MLP_MAX_ACTIVE)[v];
+    else
+        reinterpret_cast<float4 *>(t)[k] = reinterpret_cast<const float4 *>(all_t)[src];
+}
+
+// acc += loss * scale, in FP64 and in step order (one thread).
+__global__ void k_accum_loss(const float *__restrict__ loss, double *__restrict__ acc, double scale)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *acc += (double)*loss * scale;
+}
+
 // ---------------------------------------------------------------- layer 1
 // h1 = relu(b1 + sum of active rows of W1); stored FP32 (for backward) and
 // BF16 (GEMM operand).  One block of 256 threads per sample.
@@ -105,8 +131,9 @@ __global__ void k_mlp_layer1(const int16_t *__restrict__ idx, const __nv_bfloat1
 // batch) split K across gridDim.z CTAs per tile; each writes its partial
 // tile to a workspace and k_sum_splits adds the splits in a fixed order, so
 // results do not depend on scheduling.  Every mbarrier wait gives up after
-// about a second, sets *err and skips the epilogue; tensor memory is freed
-// on every path.
+// about a second, sets *err and skips the epilogue; the loads and MMAs
+// still in flight are then waited for (bounded again) and tensor memory is
+// freed on every path.
 namespace tc {
 constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4;
 constexpr u32 OPERAND_BYTES = BM * BK * 2;         // one operand chunk, 16 KB
@@ -234,7 +261,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const __grid_constant__ CUte
             load_operand<A_KMAJOR>(a, &map_a, m0, (kc0 + j) * BK, bar);
             load_operand<B_KMAJOR>(b, &map_b, n0, (kc0 + j) * BK, bar);
         };
-        for (int j = 0; j < cnt && j < STAGES; j++) issue(j);
+        int issued = 0, landed = 0;  // chunks whose loads were issued / have landed
+        for (; issued < cnt && issued < STAGES; issued++) issue(issued);
         for (int j = 0; j < cnt; j++) {
             const int st = j % STAGES;
             const u32 ph = (u32)(j / STAGES) & 1u;
@@ -242,6 +270,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const __grid_constant__ CUte
                 ok = false;
                 break;
             }
+            landed = j + 1;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const u32 a = ring + st * STAGE_BYTES, b = a + OPERAND_BYTES;
 #pragma unroll
@@ -261,13 +290,19 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const __grid_constant__ CUte
                     ok = false;
                     break;
                 }
-                issue(j + STAGES);
+                issue(issued++);
             }
         }
         // covers every MMA issued before it
-        if (ok)
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         :: "r"(smem_addr(&done)) : "memory");
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(smem_addr(&done)) : "memory");
+        if (!ok) {
+            // a wait gave up: before the CTA frees its memory, let the loads
+            // still in flight land and the issued MMAs finish (each wait
+            // bounded again)
+            for (int j = landed; j < issued; j++) mbar_wait(smem_addr(&full[j % STAGES]), (u32)(j / STAGES) & 1u);
+            mbar_wait(smem_addr(&done), 0);
+        }
     }
     if (cnt > 0 && __syncthreads_and(ok)) ok = mbar_wait(smem_addr(&done), 0);
     ok = __syncthreads_and(ok) != 0;

@@ -25,6 +25,20 @@ constexpr size_t MLP_OFF_W3 = MLP_OFF_B2 + MLP_H;
 constexpr size_t MLP_OFF_B3 = MLP_OFF_W3 + (size_t)MLP_H * MLP_OUT;
 constexpr size_t MLP_PARAMS = MLP_OFF_B3 + MLP_OUT;
 
+// An owning device array, freed when it leaves scope.
+template <class T>
+struct DeviceBuffer {
+    T *p = nullptr;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    ~DeviceBuffer()
+    {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t n) { return cudaMalloc(reinterpret_cast<void **>(&p), n * sizeof(T)); }
+};
+
 struct Mlp {
     bool ready = false;
     int max_batch = 0;
@@ -129,7 +143,10 @@ struct Mlp {
     }
 
     // Positions -> feature indices (device), for rows [0, n) of the batch buffers.
-    cudaError_t load_positions(const pb_pos *pos, int n, cudaStream_t s)
+    cudaError_t load_positions(const pb_pos *pos, int n, cudaStream_t s) { return features_to(pos, n, idx, s); }
+
+    // Feature indices of n positions (n <= max_batch) into rows [0, n) of `out`.
+    cudaError_t features_to(const pb_pos *pos, int n, int16_t *out, cudaStream_t s)
     {
         std::vector<Board> b(n);
         std::vector<uint8_t> st(n), col(n);
@@ -142,7 +159,7 @@ struct Mlp {
         if ((e = cudaMemcpyAsync(pos_b, b.data(), sizeof(Board) * n, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
         if ((e = cudaMemcpyAsync(pos_s, st.data(), n, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
         if ((e = cudaMemcpyAsync(pos_c, col.data(), n, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
-        k_features<<<(n + 255) / 256, 256, 0, s>>>(pos_b, pos_s, pos_c, n, idx);
+        k_features<<<(n + 255) / 256, 256, 0, s>>>(pos_b, pos_s, pos_c, n, out);
         return cudaGetLastError();
     }
 

@@ -34,14 +34,15 @@ def label(eng: pg.Engine, positions, depths=(1, 2, 3, 4), chunk=262144):
     """Exact perft(k) for every position, as an (n, len(depths)) float64 array."""
     out = np.zeros((len(positions), len(depths)), dtype=np.float64)
     for c0 in range(0, len(positions), chunk):
-        part = pg.pack_positions(positions[c0:c0 + chunk])
+        part = pg.pack_slice(positions, c0, c0 + chunk)
         for j, d in enumerate(depths):
             out[c0:c0 + len(part), j] = eng.perft_batch(part, d)
     return out
 
 
 def make_training_set(eng, n, seed=3):
-    pos = keep_movable(pg.random_playouts(seed, n, 0, 60))
+    """(positions as one packed array, log2(1 + perft 1..4) as float32, exact counts)."""
+    pos = pg.pack_positions(keep_movable(pg.random_playouts(seed, n, 0, 60)))
     counts = label(eng, pos)
     return pos, np.log2(1.0 + counts).astype(np.float32), counts
 

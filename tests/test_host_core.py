@@ -113,6 +113,11 @@ def test_packed_positions_and_per_root_ints():
     again = pg.pack_positions(roots)
     assert [p.key() for p in again] == [p.key() for p in roots]
     assert pg.pack_positions(packed) is packed
+    view = pg.pack_slice(packed, 10, 20)
+    assert [p.key() for p in view] == [p.key() for p in roots[10:20]]
+    assert ctypes.addressof(view) == ctypes.addressof(packed) + 10 * ctypes.sizeof(pg.Pos)  # no copy
+    assert len(pg.pack_slice(packed, 60, 80)) == 4
+    assert [p.key() for p in pg.pack_slice(roots, 10, 20)] == [p.key() for p in roots[10:20]]
     assert pg._c_ints(5, 3).tolist() == [5, 5, 5]
     assert pg._c_ints([1, 2, 3], 3).tolist() == [1, 2, 3]
     with pytest.raises(ValueError):
