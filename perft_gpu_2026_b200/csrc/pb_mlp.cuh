@@ -115,10 +115,11 @@ __global__ void k_mlp_layer1(const int16_t *__restrict__ idx, const __nv_bfloat1
 // Thread 0 keeps up to four chunks of both operands in flight with
 // cp.async.bulk.tensor loads (each stage's mbarrier counts the bytes in),
 // issues the four 128x128x16 tcgen05.mma of a chunk once its bytes have
-// landed, and commits them to the stage's second mbarrier, which it waits on
-// before loading the stage again.  Each operand keeps the layout it has in
-// global memory, as one of the two canonical 128-byte-swizzled layouts that
-// TMA writes and the MMA reads: K-major for an operand contiguous along K
+// landed, and commits them to the stage's second mbarrier; after queueing a
+// chunk's MMAs it waits on the previous chunk's commit and loads that stage
+// again, so one chunk of MMAs is always queued while loads are issued.
+// Each operand keeps the layout it has in global memory, as one of the two
+// canonical 128-byte-swizzled layouts that TMA writes and the MMA reads: K-major for an operand contiguous along K
 // (one 64 x 128 box: rows of 64 k, 8-row groups 1024 B apart; an MMA's
 // 16-k step moves the start address 32 B) or MN-major for one contiguous
 // along M or N (two 64 x 64 boxes of 64 k rows x 64 elements: 8-k groups
@@ -284,9 +285,12 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tc(const __grid_constant__ CUte
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          :: "r"(smem_addr(&empty[st])) : "memory");
-            if (j + STAGES < cnt) {
-                // the stage is free once this chunk's MMAs have read it
-                if (!mbar_wait(smem_addr(&empty[st]), ph)) {
+            if (j >= 1 && j - 1 + STAGES < cnt) {
+                // refill the previous chunk's stage once its MMAs have read
+                // it; this chunk's MMAs stay queued behind them meanwhile, so
+                // the tensor pipe does not drain while the loads are issued
+                const int jp = j - 1;
+                if (!mbar_wait(smem_addr(&empty[jp % STAGES]), (u32)(jp / STAGES) & 1u)) {
                     ok = false;
                     break;
                 }
