@@ -1346,10 +1346,13 @@ inline int plan_levels(int depth) { return std::max(depth - 2, 1); }
 
 void predicted_levels(const float *y, int depth, double *e)
 {
+    // only the predictions the levels use (exp2 is most of the planner's
+    // per-root host time)
+    const int nlev = plan_levels(depth), need = std::min(nlev, 4);
     double p[5] = {1, 0, 0, 0, 0};
-    for (int k = 1; k <= 4; k++) p[k] = std::max(exp2((double)y[k - 1]) - 1.0, 0.0);
-    double bf = p[3] > 0 ? std::max(p[4] / p[3], 1.0) : 30.0;
-    for (int k = 1; k <= plan_levels(depth); k++) e[k - 1] = k <= 4 ? p[k] : e[k - 2] * bf;
+    for (int k = 1; k <= need; k++) p[k] = std::max((double)exp2f(y[k - 1]) - 1.0, 0.0);
+    const double bf = (nlev > 4 && p[3] > 0) ? std::max(p[4] / p[3], 1.0) : 30.0;
+    for (int k = 1; k <= nlev; k++) e[k - 1] = k <= 4 ? p[k] : e[k - 2] * bf;
 }
 
 // bytes one root's batched levels take: 6 B per edge, 50 B per materialised position
