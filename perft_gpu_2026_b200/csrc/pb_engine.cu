@@ -1442,10 +1442,17 @@ int plan_and_run(pb_ctx *ctx, const pb_pos *roots, const int *depths, int n, uin
     // the items themselves stay in place)
     std::vector<u32> order(ready.size());
     for (size_t k = 0; k < order.size(); k++) order[k] = (u32)k;
-    std::sort(order.begin(), order.end(), [&](u32 a, u32 b) {
-        const PlanItem &x = ready[a], &y2 = ready[b];
-        return x.depth != y2.depth ? x.depth < y2.depth : x.bytes > y2.bytes;
-    });
+    bool one_batch = true;  // one depth and within the budget: no packing to do
+    double all_bytes = 0;
+    for (const PlanItem &it : ready) {
+        one_batch = one_batch && it.depth == ready[0].depth;
+        all_bytes += it.bytes;
+    }
+    if (!one_batch || all_bytes > budget)
+        std::sort(order.begin(), order.end(), [&](u32 a, u32 b) {
+            const PlanItem &x = ready[a], &y2 = ready[b];
+            return x.depth != y2.depth ? x.depth < y2.depth : x.bytes > y2.bytes;
+        });
     std::vector<Board> rb;
     std::vector<uint8_t> rs;
     std::vector<u64> out;

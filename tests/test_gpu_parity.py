@@ -244,6 +244,9 @@ def test_edge_depths_and_terminal_positions(gpu_engine, oracle):
             assert gpu_engine.perft_position(p, d) == oracle.perft(fen, d), (fen, d)
     roots = [pg.parse_fen(f) for f in (START, MATED, STALEMATE, START)]
     assert gpu_engine.perft_batch(roots, [0, 3, 2, 1]) == [1, 0, 0, 20]
+    # packed roots with one depth for all, and an empty batch
+    assert gpu_engine.perft_batch(pg.pack_positions(roots), 2) == [400, 0, 0, 400]
+    assert gpu_engine.perft_batch([], []) == []
 
 
 def test_batched_leaf_ranked_and_unranked_agree():

@@ -26,6 +26,13 @@ def test_planned_batch_matches_exact_counts():
     got, st = eng.perft_batch_planned(roots, depths)
     assert got == eng.perft_batch(roots, depths)
     assert st.graph_batches >= 1
+    # the packed form with one depth for all, an empty batch, terminal roots
+    packed = pg.pack_positions(roots)
+    assert eng.perft_batch_planned(packed, 4)[0] == eng.perft_batch(packed, 4)
+    empty, st0 = eng.perft_batch_planned([], [])
+    assert empty == [] and st0.batches == 0
+    mated = pg.parse_fen("rnb1kbnr/pppp1ppp/8/4p3/6Pq/5P2/PPPPP2P/RNBQKBNR w KQkq - 1 3")
+    assert eng.perft_batch_planned([mated, roots[0]], [5, 1])[0] == [0, pg.count_moves(roots[0])]
     eng.close()
 
 
