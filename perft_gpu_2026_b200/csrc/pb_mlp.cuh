@@ -111,9 +111,10 @@ __global__ void k_mlp_layer1(const int16_t *__restrict__ idx, const __nv_bfloat1
 // addresses 16-byte aligned, lda and ldb multiples of 8.
 //
 // One CTA of 128 threads per 128 x 128 tile of C (and per K split, below).
-// K advances 64 at a time through a ring of four shared-memory stages.
-// Thread 0 keeps up to four chunks of both operands in flight with
-// cp.async.bulk.tensor loads (each stage's mbarrier counts the bytes in),
+// K advances 64 at a time through a ring of three shared-memory stages (two
+// CTAs per SM).  Thread 0 keeps up to three chunks of both operands in
+// flight with cp.async.bulk.tensor loads (each stage's mbarrier counts the
+// bytes in),
 // issues the four 128x128x16 tcgen05.mma of a chunk once its bytes have
 // landed, and commits them to the stage's second mbarrier; after queueing a
 // chunk's MMAs it waits on the previous chunk's commit and loads that stage
@@ -136,7 +137,14 @@ __global__ void k_mlp_layer1(const int16_t *__restrict__ idx, const __nv_bfloat1
 // still in flight are then waited for (bounded again) and tensor memory is
 // freed on every path.
 namespace tc {
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 4;
+#ifndef PB_GEMM_STAGES
+// shared-memory stages of k_gemm_tc: 3 x 32 KB lets two CTAs share an SM, so
+// one CTA's setup and epilogue overlap the other's MMAs (16384 x 1024 x 1024:
+// 545 against 400 TFLOP/s with 4 stages and one CTA per SM)
+#define PB_GEMM_STAGES 3
+#endif
+#define PB_GEMM_CTAS_PER_SM (PB_GEMM_STAGES <= 2 ? 3 : PB_GEMM_STAGES == 3 ? 2 : 1)
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = PB_GEMM_STAGES;
 constexpr u32 OPERAND_BYTES = BM * BK * 2;         // one operand chunk, 16 KB
 constexpr u32 STAGE_BYTES = 2 * OPERAND_BYTES;     // A chunk + B chunk
 constexpr u32 SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + slack to align the ring to 1024 B
@@ -211,7 +219,7 @@ __device__ __forceinline__ u64 operand_desc(u32 base, int kk)
 // C (or, with gridDim.z > 1, split z's partial tile at C + z * split_stride)
 // for the tile (blockIdx.y, blockIdx.x) over this split's share of K.
 template <bool TA, bool TB>
-__global__ void __launch_bounds__(128, 1) k_gemm_tc(const __grid_constant__ CUtensorMap map_a,
+__global__ void __launch_bounds__(128, PB_GEMM_CTAS_PER_SM) k_gemm_tc(const __grid_constant__ CUtensorMap map_a,
                                                      const __grid_constant__ CUtensorMap map_b,
                                                      float *__restrict__ C, int ldc, size_t split_stride, int M,
                                                      int N, int K, u32 *__restrict__ err)
