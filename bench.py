@@ -24,7 +24,9 @@ Printed JSON line (rank 0):
            the reference program itself
   scheduler  (one GPU) the learned scheduler: trained on 2^20 positions,
            held-out prediction error per depth, and planned vs
-           count-then-allocate vs plain seconds on held-out roots at depths 4..7
+           count-then-allocate vs plain seconds on held-out roots at depths 4..7;
+           `gemm_roofline`: the network's tcgen05 GEMM against the measured
+           dense BF16 peak
   positions  (one GPU) positions/s on 4096 uneven roots at perft 5: plain
            per-root calls, count-then-allocate batch, learned planner
   tt_run   (one GPU) perft 10 of the 2-ply seed-4 position with 150 GB of
@@ -314,6 +316,42 @@ def scheduler_section(pg, eng, train_n=1 << 20, eval_n=16384, timed_n=1024):
                       "timing": "host wall clock around the public call, one run each"}}
 
 
+def gemm_section(eng, reps=50):
+    """The scheduler network's tcgen05 GEMM against the measured dense BF16
+    peak (burst figure: each product is timed alone): layer 2's forward
+    product at a 4096-sample batch, its weight gradient (K split over 16
+    CTAs per tile), and a large product that the network does not need, for
+    the kernel's ceiling.  CUDA events around `reps` launches after one
+    checked launch; the check compares 64 rows of C with a float64 product
+    of the same BF16 values."""
+    import numpy as np
+
+    peaks, kind = _peaks()
+    peak = peaks.get("bf16_tflops", 1590.0)
+    rng = np.random.default_rng(7)
+    out = {"unit": "TFLOP/s", "peak": peak, "peak_source": f"bf16_tflops ({kind})",
+           "timing": f"CUDA events, mean of {reps} launches after one checked launch"}
+    shapes = (("layer2_forward", 4096, 256, 256, False, False),
+              ("layer2_weight_gradient", 256, 256, 4096, True, False),
+              ("large_8192x2048x2048", 8192, 2048, 2048, False, False))
+    for name, m, n, k, ta, tb in shapes:
+        a = rng.uniform(-1, 1, size=m * k).astype(np.float32)
+        b = rng.uniform(-1, 1, size=k * n).astype(np.float32)
+        ab = ((a.view(np.uint32) + 0x8000) >> 16).astype(np.uint16)
+        bb = ((b.view(np.uint32) + 0x8000) >> 16).astype(np.uint16)
+        c, ms = eng.selftest_gemm(ab, bb, ta, tb, m, n, k, reps=reps)
+        av = (ab.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+        bv = (bb.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+        am = av.reshape(k, m).T if ta else av.reshape(m, k)
+        bm = bv.reshape(n, k).T if tb else bv.reshape(k, n)
+        rows = rng.choice(m, size=min(64, m), replace=False)
+        err = float(np.abs(c[rows] - am[rows] @ bm).max())
+        assert err <= 1e-5 * k + 1e-4, (name, err)
+        tf = 2.0 * m * n * k / (ms * 1e-3) / 1e12
+        out[name] = {"m": m, "n": n, "k": k, "ms": ms, "achieved": tf, "frac": tf / peak, "max_abs_err": err}
+    return out
+
+
 def positions_section(pg, eng, reps):
     """Positions/s on 4096 uneven roots (playouts of 6..40 plies, splitmix64
     seed 2), perft 5 each, three ways through the public API (roots in host
@@ -575,6 +613,7 @@ def main():
                 "gpu_launches": int(kernels), "clocks": clocks, "roofline": roofline}
         if world == 1 and not args.no_positions:
             line["scheduler"] = scheduler_section(pg, eng)
+            line["scheduler"]["gemm_roofline"] = gemm_section(eng)
             line["positions"] = positions_section(pg, eng, reps=min(args.steps, 3))
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_baseline(child_fens, depth)
